@@ -1,0 +1,203 @@
+/* cmfw.h -- C ABI of the B200 pFq Conservative Matrix Field walk engine.
+ *
+ * Plain pointers and sizes only. Every walk entry point takes DEVICE
+ * pointers and a CUDA stream (as `void *`, NULL = legacy default stream),
+ * enqueues its kernels and returns without synchronising, except where a
+ * comment says otherwise. The `_host` entry points take HOST buffers, copy
+ * them to the device, run, copy the results back and synchronise.
+ *
+ * The reference (VesterlundCoder/RamanujanDreams-CUDA) exposes no library:
+ * its boundary is three programs, each of which builds inputs, launches one
+ * kernel `walk_kernel_<variant><<<grid, block>>>(inputs, results, desc, N, h,
+ * n_traj[, n_primes])` and writes JSON. The entry points below replace those
+ * launches (cited per function); the records keep the reference's byte
+ * layout so that the reference's own input builders can feed them.
+ *
+ * Threading: calls are thread-safe; calls on different streams may overlap.
+ * Errors: every entry point returns a cmfw_status; cmfw_last_error() gives
+ * a message for the calling thread's most recent failure. Per-trajectory
+ * failures are not call failures: they set `valid = 0` in the record, and
+ * the optional status array says why (cmfw_traj_status).
+ */
+#ifndef CMFW_H
+#define CMFW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMFW_MAX_DIM 8    /* cmf_pfq.cuh:36  MAX_DIM  */
+#define CMFW_MAX_AXES 16  /* cmf_pfq.cuh:38  MAX_AXES */
+#define CMFW_MAX_COMPAT_MODULI 64   /* cmf_walk_rns.cu:23 MAX_PRIMES */
+#define CMFW_MAX_EXACT_PRIMES 4096
+
+typedef enum {
+    CMFW_OK = 0,
+    CMFW_EINVAL = 1,      /* argument out of the supported range */
+    CMFW_ECUDA = 2,       /* a CUDA runtime call failed */
+    CMFW_ENOMEM = 3,      /* device or host allocation failed */
+    CMFW_ETIMEOUT = 4,    /* a bounded device wait gave up */
+    CMFW_EUNSUPPORTED = 5 /* built without the requested kernel */
+} cmfw_status;
+
+/* Why a trajectory is invalid (values of the optional status array). */
+typedef enum {
+    CMFW_TRAJ_OK = 0,
+    CMFW_TRAJ_SINGULAR_LEAD = 1,   /* companion lead coefficient ~ 0 (cmf_pfq.cuh:173) */
+    CMFW_TRAJ_SINGULAR_DENOM = 2,  /* axis denominator ~ 0 (cmf_pfq.cuh:193) */
+    CMFW_TRAJ_SINGULAR_SOLVE = 3,  /* inverse-step scalar solve ~ 0 (cmf_pfq.cuh:225) */
+    CMFW_TRAJ_NONFINITE = 4,       /* non-finite or all-zero walk matrix (cmf_pfq.cuh:109) */
+    CMFW_TRAJ_BAD_DEPTH = 5,       /* N <= 0, h <= 0 or N - 2h <= 0 (cmf_pfq.cuh:352) */
+    CMFW_TRAJ_STEP_CAP = 6,        /* |dir| beyond CMFW_MAX_DIR_COMPONENT */
+    CMFW_TRAJ_MODULUS_ZERO = 7,    /* exact walk: a divisor vanished modulo this prime */
+    CMFW_TRAJ_NOT_INTEGRAL = 8     /* exact walk: a start coordinate is not an integer */
+} cmfw_traj_status;
+
+/* Largest |dir[a]| a trajectory may use; larger components mark the
+ * trajectory CMFW_TRAJ_STEP_CAP instead of walking (bounded device loops). */
+#define CMFW_MAX_DIR_COMPONENT 4096
+
+/* CMFDesc (cmf_pfq.cuh:41-47), same field order and layout. */
+typedef struct {
+    int p;      /* numerator parameters (x axes), 1..8 */
+    int q;      /* denominator parameters (y axes), 0..7 */
+    int rank;   /* walk-matrix dimension, 2..8 */
+    int naxes;  /* p + q */
+    double z;
+} cmfw_desc;
+
+/* TrajectoryInput / DF64Input / RNSInput (cmf_walk_f64.cu:36-39): 192 bytes. */
+typedef struct {
+    int dir[CMFW_MAX_AXES];       /* lattice direction, x axes then y axes */
+    double start[CMFW_MAX_AXES];  /* start position (x_1..x_p, y_1..y_q) */
+} cmfw_traj_in;
+
+/* DF64Result / RNSResult (cmf_walk_df64.cu:293-302): 56 bytes. The f64
+ * program's TrajectoryResult (cmf_walk_f64.cu:41-51) is this record plus a
+ * trailing, never-written `elapsed_ms`. */
+typedef struct {
+    double limit;      /* first Aitken limit, else first candidate */
+    double delta;      /* irrationality-measure estimate */
+    double p, q;       /* M[0][rank-1], M[1][rank-1] of the normalised matrix at depth N */
+    double precision;  /* -log10 |p_N/q_N - p_{N-h}/q_{N-h}| */
+    double log_scale;  /* log of the normalisation scale at depth N */
+    int valid;         /* 1 = walked all N steps */
+    int n_limits;      /* limit candidates found (capped at 256) */
+} cmfw_traj_out;
+
+/* Launch options; a zeroed struct (or NULL) selects the defaults. */
+typedef struct {
+    int block_size;        /* threads per block; 0 = tuned default */
+    int flags;             /* CMFW_F_* below */
+    uint8_t *d_status;     /* optional per-trajectory cmfw_traj_status */
+    void *d_workspace;     /* optional caller-owned scratch (see *_workspace_bytes) */
+    size_t workspace_bytes;
+    int *d_limit_src;      /* optional per-trajectory source of `limit`:
+                              (method << 12) | (i << 8) | (j << 4) | column for
+                              the ratio M[i][column] / M[j][column]; method 1 =
+                              Aitken, 0 = raw ratio; -1 = no candidate */
+} cmfw_launch;
+
+/* df64 arithmetic: reproduce the reference's float-reciprocal semantics
+ * (cmf_walk_df64.cu:110-113, 138-153, 184, 194, 210). Default: accurate
+ * float-float with refined reciprocals and power-of-two renormalisation. */
+#define CMFW_F_DF64_COMPAT 0x1
+/* RNS compat: evaluate the column polynomial with separately rounded
+ * products and sums (the reference compiled for a CPU) instead of fused
+ * multiply-adds (the reference compiled by nvcc). */
+#define CMFW_F_UNFUSED_COLUMN 0x2
+
+/* ---- descriptors and library state -------------------------------- */
+
+const char *cmfw_version(void);
+const char *cmfw_last_error(void);
+/* make_cmf_desc (cmf_pfq.cuh:50-61). */
+cmfw_desc cmfw_make_desc(int p, int q, double z);
+/* CMFW_OK when desc is within the supported range (p <= 8, q <= 7,
+ * 2 <= rank <= 8, naxes == p + q). */
+cmfw_status cmfw_check_desc(const cmfw_desc *desc);
+
+/* Scratch a walk call needs when the caller supplies d_workspace; when
+ * d_workspace is NULL the library uses its own per-device buffer. */
+size_t cmfw_walk_workspace_bytes(const cmfw_desc *desc, int n_traj);
+
+/* ---- plain walks (device buffers) --------------------------------- */
+
+/* Replaces walk_kernel_f64<<<...>>>(inputs, results, desc, N, h, n_traj)
+ * (cmf_walk_f64.cu:94-96, 228). */
+cmfw_status cmfw_walk_f64(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_traj_out *d_out,
+                          int n_traj, int N, int h, const cmfw_launch *launch, void *stream);
+
+/* Replaces walk_kernel_df64<<<...>>>(inputs, results, desc, N, h, n_traj)
+ * (cmf_walk_df64.cu:304-306, 410). */
+cmfw_status cmfw_walk_df64(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_traj_out *d_out,
+                           int n_traj, int N, int h, const cmfw_launch *launch, void *stream);
+
+/* Replaces walk_kernel_rns<<<...>>>(inputs, results, desc, N, h, n_traj,
+ * n_primes) (cmf_walk_rns.cu:260-262, 381). Residues are bit-identical to
+ * the reference's: same 64-entry modulus table, same rounded column, same
+ * 100-step two-modulus reconstruction. 1 <= n_primes <= 64. */
+cmfw_status cmfw_walk_rns(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_traj_out *d_out,
+                          int n_traj, int N, int h, int n_primes, const cmfw_launch *launch,
+                          void *stream);
+
+/* Residue matrices of the compat RNS walk after `steps` trajectory steps
+ * (the state inside walk_kernel_rns, cmf_walk_rns.cu:281-298, which the
+ * reference never exports). d_res: n_traj * n_primes * rank * rank uint32,
+ * trajectory-major, then modulus, row, column. d_ok: n_traj ints. */
+cmfw_status cmfw_rns_trace(const cmfw_desc *desc, const cmfw_traj_in *d_in, int n_traj, int N,
+                           int h, int n_primes, int steps, int flags, uint32_t *d_res, int *d_ok,
+                           void *stream);
+
+/* ---- exact walk (no reference counterpart: the reference's RNS rounds) --
+ * The walk product is kept exactly as rational residues modulo K primes
+ * (one warp lane per prime, Montgomery arithmetic): each step multiplies by
+ * I + C/a or its inverse with C's column -d/lead taken mod the prime. At
+ * the snapshot depths N-2h, N-h, N two entries of one column are written,
+ * M[i][c] and M[j][c] (by default i = 0, j = 1, c = rank-1: p and q), so
+ * that their ratio (and each entry) can be recovered by CRT and rational
+ * reconstruction on the host.
+ * d_primes: K distinct odd primes below 2^31. d_pairs: optional n_traj
+ * packed (i << 8) | (j << 4) | c selectors (the low 12 bits of
+ * cmfw_launch.d_limit_src values are accepted as they are). d_res: n_traj
+ * * 3 * 2 * K uint32 (trajectory, snapshot, {M[i][c], M[j][c]}, prime).
+ * d_prime_ok: n_traj * K bytes, 1 where no divisor vanished modulo that
+ * prime; 0 for every prime when the trajectory cannot be walked exactly
+ * (bad depth, direction cap, non-integral start). */
+cmfw_status cmfw_exact_residues(const cmfw_desc *desc, const cmfw_traj_in *d_in, int n_traj,
+                                int N, int h, const uint32_t *d_primes, int K, const int *d_pairs,
+                                uint32_t *d_res, uint8_t *d_prime_ok, void *stream);
+
+/* ---- input records -------------------------------------------------- */
+
+/* The reference programs' input records for `mode` (0 = limit, 1 = delta)
+ * and `use_zeta`, byte for byte as run_benchmark() builds them
+ * (cmf_walk_f64.cu:166-199 with the generators of cmf_walk_f64.cu:61-91,
+ * std::mt19937_64 seeded 42, including their write strides). */
+cmfw_status cmfw_reference_inputs(int p, int q, int n_traj, int mode, int use_zeta, cmfw_traj_in *h_out);
+/* n outputs of std::mt19937_64(seed), for seeded workload generators. */
+void cmfw_mt64_fill(uint64_t seed, uint64_t *out, size_t n);
+
+/* ---- host-buffer convenience (what the drop-in programs call) ------- */
+
+typedef enum { CMFW_VARIANT_F64 = 0, CMFW_VARIANT_DF64 = 1, CMFW_VARIANT_RNS = 2 } cmfw_variant;
+
+/* Copies h_in to the device, runs the variant, copies results to h_out and
+ * synchronises. *kernel_ms (optional) receives the event-timed duration of
+ * the walk kernels alone; *total_ms (optional) the copies included. */
+cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cmfw_traj_in *h_in,
+                           cmfw_traj_out *h_out, int n_traj, int N, int h, int n_primes,
+                           const cmfw_launch *launch, float *kernel_ms, float *total_ms);
+
+/* Device properties line for the programs' stderr banner. */
+cmfw_status cmfw_device_banner(char *buf, size_t size);
+/* cudaMemGetInfo of the current device (device-wide, all processes). */
+cmfw_status cmfw_device_meminfo(size_t *free_bytes, size_t *total_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CMFW_H */

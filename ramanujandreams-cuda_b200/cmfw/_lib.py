@@ -1,0 +1,99 @@
+"""Loads libcmfw.so (the C ABI of include/cmfw.h) and declares its signatures.
+
+The library is built in-tree by ``make -C ramanujandreams-cuda_b200``; there
+is no fallback implementation: if the library is missing, every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libcmfw.so")
+BIN_DIR = os.path.join(PKG_ROOT, "bin")
+
+IN_DTYPE = np.dtype([("dir", "<i4", 16), ("start", "<f8", 16)])
+OUT_DTYPE = np.dtype([("limit", "<f8"), ("delta", "<f8"), ("p", "<f8"), ("q", "<f8"),
+                      ("precision", "<f8"), ("log_scale", "<f8"), ("valid", "<i4"),
+                      ("n_limits", "<i4")])
+assert IN_DTYPE.itemsize == 192 and OUT_DTYPE.itemsize == 56
+
+CMFW_OK = 0
+STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ETIMEOUT", 5: "EUNSUPPORTED"}
+TRAJ_STATUS = {0: "ok", 1: "singular_lead", 2: "singular_denom", 3: "singular_solve",
+               4: "nonfinite", 5: "bad_depth", 6: "step_cap", 7: "modulus_zero",
+               8: "not_integral"}
+
+F_DF64_COMPAT = 0x1
+F_UNFUSED_COLUMN = 0x2
+
+VARIANTS = {"f64": 0, "df64": 1, "rns": 2}
+
+# Every symbol include/cmfw.h declares.
+EXPORTS = [
+    "cmfw_version", "cmfw_last_error", "cmfw_make_desc", "cmfw_check_desc",
+    "cmfw_walk_workspace_bytes", "cmfw_walk_f64", "cmfw_walk_df64", "cmfw_walk_rns",
+    "cmfw_rns_trace", "cmfw_exact_residues", "cmfw_reference_inputs", "cmfw_mt64_fill",
+    "cmfw_walk_host", "cmfw_device_banner", "cmfw_device_meminfo",
+]
+
+
+class CmfwError(RuntimeError):
+    """A cmfw_* call returned a status other than CMFW_OK."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Desc(ctypes.Structure):
+    """cmfw_desc (CMFDesc, cmf_pfq.cuh:41-47)."""
+    _fields_ = [("p", ctypes.c_int), ("q", ctypes.c_int), ("rank", ctypes.c_int),
+                ("naxes", ctypes.c_int), ("z", ctypes.c_double)]
+
+
+class Launch(ctypes.Structure):
+    _fields_ = [("block_size", ctypes.c_int), ("flags", ctypes.c_int),
+                ("d_status", ctypes.c_void_p), ("d_workspace", ctypes.c_void_p),
+                ("workspace_bytes", ctypes.c_size_t), ("d_limit_src", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PKG_ROOT}` "
+                               "(the CMF walk has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ci, cd, cs = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+        P = ctypes.POINTER
+        L.cmfw_version.restype = ctypes.c_char_p
+        L.cmfw_last_error.restype = ctypes.c_char_p
+        L.cmfw_make_desc.restype = Desc
+        L.cmfw_make_desc.argtypes = [ci, ci, cd]
+        L.cmfw_check_desc.argtypes = [P(Desc)]
+        L.cmfw_walk_workspace_bytes.restype = cs
+        L.cmfw_walk_workspace_bytes.argtypes = [P(Desc), ci]
+        for name in ("cmfw_walk_f64", "cmfw_walk_df64"):
+            getattr(L, name).argtypes = [P(Desc), vp, vp, ci, ci, ci, P(Launch), vp]
+        L.cmfw_walk_rns.argtypes = [P(Desc), vp, vp, ci, ci, ci, ci, P(Launch), vp]
+        L.cmfw_rns_trace.argtypes = [P(Desc), vp, ci, ci, ci, ci, ci, ci, vp, vp, vp]
+        L.cmfw_exact_residues.argtypes = [P(Desc), vp, ci, ci, ci, vp, ci, vp, vp, vp, vp]
+        L.cmfw_reference_inputs.argtypes = [ci, ci, ci, ci, ci, vp]
+        L.cmfw_mt64_fill.argtypes = [ctypes.c_uint64, vp, cs]
+        L.cmfw_mt64_fill.restype = None
+        L.cmfw_walk_host.argtypes = [ci, P(Desc), vp, vp, ci, ci, ci, ci, P(Launch),
+                                     P(ctypes.c_float), P(ctypes.c_float)]
+        L.cmfw_device_banner.argtypes = [ctypes.c_char_p, cs]
+        L.cmfw_device_meminfo.argtypes = [P(cs), P(cs)]
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != CMFW_OK:
+        raise CmfwError(status, lib().cmfw_last_error().decode())

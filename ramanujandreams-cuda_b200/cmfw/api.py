@@ -1,0 +1,177 @@
+"""Python host interface over the C ABI.
+
+Mirrors the reference's per-variant operation -- build trajectory records,
+run one walk over them, read back one result record per trajectory
+(cmf_walk_{f64,df64,rns}.cu run_benchmark) -- with the walk itself always on
+the GPU through libcmfw.so. torch supplies device memory and streams only.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import (IN_DTYPE, OUT_DTYPE, VARIANTS, Desc, Launch, check, lib)
+
+
+def make_desc(p, q, z):
+    """cmfw_make_desc (make_cmf_desc, cmf_pfq.cuh:50-61)."""
+    return lib().cmfw_make_desc(int(p), int(q), float(z))
+
+
+def check_desc(desc):
+    check(lib().cmfw_check_desc(ctypes.byref(desc)))
+
+
+def version():
+    return lib().cmfw_version().decode()
+
+
+def reference_inputs(p, q, n, mode, use_zeta):
+    """Input records exactly as the reference programs build them."""
+    out = np.zeros(n, dtype=IN_DTYPE)
+    check(lib().cmfw_reference_inputs(p, q, n, int(mode), int(bool(use_zeta)),
+                                      out.ctypes.data_as(ctypes.c_void_p)))
+    return out
+
+
+def mt64(seed, n):
+    """n outputs of std::mt19937_64(seed)."""
+    out = np.zeros(n, dtype=np.uint64)
+    lib().cmfw_mt64_fill(ctypes.c_uint64(seed), out.ctypes.data_as(ctypes.c_void_p), n)
+    return out
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_handle(stream):
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def to_device(records):
+    """Copy IN_DTYPE records (numpy) to a device uint8 tensor of n x 192 bytes."""
+    torch = _torch()
+    arr = np.ascontiguousarray(records, dtype=IN_DTYPE)
+    return torch.from_numpy(arr.view(np.uint8).reshape(len(arr), IN_DTYPE.itemsize)).cuda()
+
+
+def out_buffer(n):
+    torch = _torch()
+    return torch.empty((max(n, 1), OUT_DTYPE.itemsize), dtype=torch.uint8, device="cuda")
+
+
+def records_from_device(buf, n):
+    host = buf[:n].cpu().numpy()
+    return host.reshape(-1).view(OUT_DTYPE).copy()
+
+
+def launch_walk(variant, desc, d_in, d_out, n, N, h, n_primes=8, flags=0, block_size=0,
+                d_status=None, d_limit_src=None, d_workspace=None, stream=None):
+    """Enqueue one walk on device buffers (torch tensors); no synchronisation."""
+    L = lib()
+    launch = Launch()
+    launch.block_size = block_size
+    launch.flags = flags
+    launch.d_status = d_status.data_ptr() if d_status is not None else None
+    launch.d_limit_src = d_limit_src.data_ptr() if d_limit_src is not None else None
+    if d_workspace is not None:
+        launch.d_workspace = d_workspace.data_ptr()
+        launch.workspace_bytes = d_workspace.numel() * d_workspace.element_size()
+    s = _stream_handle(stream)
+    pin, pout = ctypes.c_void_p(d_in.data_ptr()), ctypes.c_void_p(d_out.data_ptr())
+    if variant == "f64":
+        st = L.cmfw_walk_f64(ctypes.byref(desc), pin, pout, n, N, h, ctypes.byref(launch), s)
+    elif variant == "df64":
+        st = L.cmfw_walk_df64(ctypes.byref(desc), pin, pout, n, N, h, ctypes.byref(launch), s)
+    elif variant == "rns":
+        st = L.cmfw_walk_rns(ctypes.byref(desc), pin, pout, n, N, h, n_primes, ctypes.byref(launch), s)
+    else:
+        raise ValueError(f"unknown variant {variant!r}")
+    check(st)
+
+
+def walk(variant, desc, records, N, h, n_primes=8, flags=0, block_size=0, with_status=False,
+         with_limit_src=False):
+    """Walk numpy records on the GPU and return numpy result records.
+
+    Returns OUT_DTYPE records, plus the per-trajectory status codes and/or
+    limit-source codes when requested.
+    """
+    torch = _torch()
+    n = len(records)
+    d_in = to_device(records) if n else torch.empty((1, 192), dtype=torch.uint8, device="cuda")
+    d_out = out_buffer(n)
+    d_status = torch.empty(max(n, 1), dtype=torch.uint8, device="cuda") if with_status else None
+    d_src = torch.empty(max(n, 1), dtype=torch.int32, device="cuda") if with_limit_src else None
+    launch_walk(variant, desc, d_in, d_out, n, N, h, n_primes, flags, block_size, d_status, d_src)
+    torch.cuda.synchronize()
+    res = [records_from_device(d_out, n)]
+    if with_status:
+        res.append(d_status[:n].cpu().numpy())
+    if with_limit_src:
+        res.append(d_src[:n].cpu().numpy())
+    return res[0] if len(res) == 1 else tuple(res)
+
+
+def walk_host(variant, desc, records, N, h, n_primes=8, flags=0, block_size=0):
+    """cmfw_walk_host: host buffers in and out; returns (results, kernel_ms, total_ms)."""
+    recs = np.ascontiguousarray(records, dtype=IN_DTYPE)
+    n = len(recs)
+    out = np.zeros(max(n, 1), dtype=OUT_DTYPE)
+    launch = Launch()
+    launch.block_size = block_size
+    launch.flags = flags
+    kms, tms = ctypes.c_float(0), ctypes.c_float(0)
+    check(lib().cmfw_walk_host(VARIANTS[variant], ctypes.byref(desc),
+                               recs.ctypes.data_as(ctypes.c_void_p),
+                               out.ctypes.data_as(ctypes.c_void_p), n, N, h, n_primes,
+                               ctypes.byref(launch), ctypes.byref(kms), ctypes.byref(tms)))
+    return out[:n], kms.value, tms.value
+
+
+def rns_trace(desc, records, N, h, n_primes, steps, flags=0):
+    """Compat-RNS residue matrices after `steps` steps: (res[n, K, rank, rank], ok[n])."""
+    torch = _torch()
+    n = len(records)
+    d_in = to_device(records)
+    r = desc.rank
+    d_res = torch.zeros((n, n_primes, r, r), dtype=torch.int32, device="cuda")
+    d_ok = torch.zeros(n, dtype=torch.int32, device="cuda")
+    check(lib().cmfw_rns_trace(ctypes.byref(desc), ctypes.c_void_p(d_in.data_ptr()), n, N, h,
+                               n_primes, steps, flags, ctypes.c_void_p(d_res.data_ptr()),
+                               ctypes.c_void_p(d_ok.data_ptr()), _stream_handle(None)))
+    torch.cuda.synchronize()
+    return d_res.cpu().numpy().view(np.uint32), d_ok.cpu().numpy().astype(bool)
+
+
+def exact_residues(desc, records, N, h, primes, pairs=None, d_in=None):
+    """Exact walk residues: (res[n, 3, 2, K] uint32, prime_ok[n, K] bool)."""
+    torch = _torch()
+    n = len(records) if d_in is None else d_in.shape[0]
+    if d_in is None:
+        d_in = to_device(records)
+    primes = np.ascontiguousarray(primes, dtype=np.uint32)
+    K = len(primes)
+    d_primes = torch.from_numpy(primes.view(np.int32)).cuda()
+    d_res = torch.zeros((n, 3, 2, K), dtype=torch.int32, device="cuda")
+    d_ok = torch.zeros((n, K), dtype=torch.uint8, device="cuda")
+    d_pairs = None
+    if pairs is not None:
+        d_pairs = torch.from_numpy(np.ascontiguousarray(pairs, dtype=np.int32)).cuda()
+    check(lib().cmfw_exact_residues(
+        ctypes.byref(desc), ctypes.c_void_p(d_in.data_ptr()), n, N, h,
+        ctypes.c_void_p(d_primes.data_ptr()), K,
+        ctypes.c_void_p(d_pairs.data_ptr()) if d_pairs is not None else None,
+        ctypes.c_void_p(d_res.data_ptr()), ctypes.c_void_p(d_ok.data_ptr()), _stream_handle(None)))
+    torch.cuda.synchronize()
+    return d_res.cpu().numpy().view(np.uint32), d_ok.cpu().numpy().astype(bool)
+
+
+def device_banner():
+    buf = ctypes.create_string_buffer(512)
+    check(lib().cmfw_device_banner(buf, 512))
+    return buf.value.decode()

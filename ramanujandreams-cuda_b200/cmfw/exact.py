@@ -1,0 +1,205 @@
+"""Exact verification of floating-point walk results.
+
+The GPU exact walk (cmfw_exact_residues) keeps the walk product as rational
+residues modulo K primes. Here the residues of two entries of one column at
+the three snapshot depths become exact rationals: per prime the ratio
+a * b^-1, Chinese remaindering over the primes, then rational reconstruction
+(Wang's half-extended-Euclid bound sqrt(P/2)) checked against held-out
+primes. When the check fails the walk is rerun with four times the primes.
+
+"Verified" means: the floating-point walk is valid, the exact walk is valid,
+and the reported limit agrees with the exact value of the same estimator
+(the same matrix ratio, Aitken or raw) within the stated relative tolerance.
+"""
+from fractions import Fraction
+import math
+
+import numpy as np
+
+from . import api
+
+CHECK_PRIMES = 4
+_prime_cache = []
+
+
+def _is_prime_u32(n):
+    if n < 2:
+        return False
+    for sp in (2, 3, 5, 7, 11, 13):
+        if n % sp == 0:
+            return n == sp
+    d, s = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        s += 1
+    for a in (2, 3, 5, 7):  # deterministic below 3.2e9
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(s - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def primes_below_2_31(K):
+    """The K largest primes below 2^31, descending."""
+    if len(_prime_cache) < K:
+        c = (_prime_cache[-1] - 2) if _prime_cache else (1 << 31) - 1
+        while len(_prime_cache) < K:
+            if _is_prime_u32(c):
+                _prime_cache.append(c)
+            c -= 2
+    return np.array(_prime_cache[:K], dtype=np.uint64)
+
+
+def _vec_pow(b, e, p):
+    """b^e mod p elementwise (uint64 arrays, p < 2^31)."""
+    r = np.ones_like(b)
+    b = b % p
+    e = e.copy()
+    while np.any(e):
+        odd = (e & 1).astype(bool)
+        r = np.where(odd, (r * b) % p, r)
+        b = (b * b) % p
+        e >>= 1
+    return r
+
+
+def _rational_reconstruct(u, m):
+    """a/b with a = u*b mod m, |a|, b <= sqrt(m/2), or None."""
+    bound = math.isqrt(m // 2)
+    r0, r1 = m, u % m
+    t0, t1 = 0, 1
+    while r1 > bound:
+        qq = r0 // r1
+        r0, r1 = r1, r0 - qq * r1
+        t0, t1 = t1, t0 - qq * t1
+    if t1 == 0 or abs(t1) > bound or math.gcd(r1, abs(t1)) != 1:
+        return None
+    if t1 < 0:
+        r1, t1 = -r1, -t1
+    return Fraction(r1, t1)
+
+
+def _ratio_from_residues(a, b, ok, primes):
+    """Exact a/b from residues a[K], b[K] modulo `primes`.
+
+    Returns a Fraction, "inf" when b vanishes modulo every surviving prime
+    (b == 0 exactly), or None when the primes do not determine the value
+    (too few, or the reconstruction fails the held-out check).
+    """
+    p = primes
+    usable = ok & (b != 0)
+    if not ok.any():
+        return None
+    if not usable.any():
+        return "inf"
+    use = np.nonzero(usable)[0]
+    if len(use) < CHECK_PRIMES + 2:
+        return None
+    bi = _vec_pow(b.astype(np.uint64), p - 2, p)
+    u = (a.astype(np.uint64) * bi) % p
+    crt, chk = use[:-CHECK_PRIMES], use[-CHECK_PRIMES:]
+    X, M = 0, 1
+    for k in crt:  # incremental Chinese remaindering
+        pk, uk = int(p[k]), int(u[k])
+        X += M * (((uk - X) * pow(M % pk, -1, pk)) % pk)
+        M *= pk
+    fr = _rational_reconstruct(X, M)
+    if fr is None:
+        return None
+    for k in chk:
+        pk = int(p[k])
+        if (fr.numerator - int(u[k]) * fr.denominator) % pk != 0:
+            return None
+    return fr
+
+
+def exact_ratios(desc, records, N, h, pairs=None, K0=64, K_max=4096):
+    """Exact snapshot ratios M[i][c]/M[j][c] at N-2h, N-h, N per trajectory.
+
+    Returns (ratios, K_used): ratios[t] is a list of three Fractions ("inf"
+    where the denominator is exactly zero), or None where the exact walk is
+    invalid (a divisor vanished for every prime).
+    """
+    n = len(records)
+    ratios = [None] * n
+    K_used = np.zeros(n, dtype=np.int64)
+    todo = np.arange(n)
+    K = K0
+    while len(todo) and K <= K_max:
+        primes = primes_below_2_31(K)
+        sub = records[todo]
+        sub_pairs = None if pairs is None else np.asarray(pairs)[todo]
+        res, ok = api.exact_residues(desc, sub, N, h, primes.astype(np.uint32), sub_pairs)
+        retry = []
+        for li, t in enumerate(todo):
+            if not ok[li].any():
+                ratios[t] = None
+                K_used[t] = K
+                continue
+            rs = []
+            for s in range(3):
+                r = _ratio_from_residues(res[li, s, 0], res[li, s, 1], ok[li], primes)
+                if r is None:
+                    break
+                rs.append(r)
+            if len(rs) < 3:
+                retry.append(t)
+            else:
+                ratios[t] = rs
+                K_used[t] = K
+        todo = np.array(retry, dtype=np.int64)
+        K *= 4
+    for t in todo:
+        K_used[t] = -1  # not determined within K_max primes
+    return ratios, K_used
+
+
+def exact_estimator(rs, method):
+    """The limit estimator of the reference's reduction on exact ratios."""
+    if rs is None or any(r == "inf" for r in rs):
+        return None
+    r1, r2, r3 = rs
+    if method == 1:
+        den = r1 - 2 * r2 + r3
+        if den != 0:
+            return r3 - (r2 - r3) ** 2 / den
+    return r3
+
+
+def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=64):
+    """Per-trajectory exact check of float results.
+
+    Returns a dict of arrays: verified (bool), rel_err (float, nan where not
+    comparable), exact_limit (float), K (primes used).
+    """
+    n = len(records)
+    valid = np.asarray(results["valid"]) == 1
+    src = np.asarray(limit_src)
+    idx = np.nonzero(valid & (src >= 0))[0]
+    verified = np.zeros(n, dtype=bool)
+    rel = np.full(n, np.nan)
+    exact_limit = np.full(n, np.nan)
+    Ks = np.zeros(n, dtype=np.int64)
+    if len(idx):
+        ratios, K_used = exact_ratios(desc, records[idx], N, h, pairs=src[idx] & 0xFFF, K0=K0)
+        for li, t in enumerate(idx):
+            Ks[t] = K_used[li]
+            L = exact_estimator(ratios[li], (int(src[t]) >> 12) & 1)
+            if L is None:
+                continue
+            Lf = float(L)
+            exact_limit[t] = Lf
+            lf = float(results["limit"][t])
+            if Lf == 0.0:
+                err = abs(lf)
+            else:
+                err = abs(Fraction(lf) - L) / abs(L)
+            rel[t] = float(err)
+            verified[t] = rel[t] <= rtol
+    return {"verified": verified, "rel_err": rel, "exact_limit": exact_limit, "K": Ks}
