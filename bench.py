@@ -1,0 +1,362 @@
+#!/usr/bin/env python3
+"""Benchmark: 6F5 zeta delta search, N = 1000, verified trajectories per second.
+
+Workload (one "step" = one walk of the whole batch): 6F5 at the zeta point
+(x = 1^6, y = 2^5), z = 1, rank 5, 10,000 directions over the 11 axes with
+components uniform in 0..3, not all zero (std::mt19937_64, seeded), N = 1000,
+h = 50, walked in f64 on the GPU. After the timed region every valid result
+is checked against the exact walk (rational residues modulo up to 4096
+primes, CRT and rational reconstruction); a trajectory is *verified* when its
+limit is within 1e-10 relative of the exact value of the same estimator.
+
+value = verified trajectories per second of walk-kernel time (whole job:
+sum over ranks / max over ranks). e2e = the same through cmfw_walk_host with
+pinned host records (copies in the timed region). Under torchrun each rank
+walks its own seeded batch (weak scaling; no collective on the data path,
+one small gather of counters at the end).
+
+--impl reference times the reference's own kernel bodies compiled for the
+host (oracle/_ref, OpenMP over all host cores) on the same batch.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "ramanujandreams-cuda_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "6F5 N=1000 verified traj/s on 1 B200 at <=1e-10 vs RNS"
+P, Q, Z, N, H, NTRAJ = 6, 5, 1.0, 1000, 50, 10000
+SEED = 20261203
+RTOL = 1e-10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cmfw", choices=["cmfw", "reference"])
+    ap.add_argument("--variant", default="f64", choices=["f64", "df64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def workload(rank):
+    import cmfw.workloads as wl
+    return wl.zeta_directions(P, Q, NTRAJ, SEED + rank)
+
+
+def flops_per_traj(records, valid, dim):
+    """Algorithmic flops of a valid walk, by the per-axis-step count of the
+    reference update (FMA = 2): column 1.5p(p+1) + 1.5q(q+1) + p + q + 2,
+    forward update 4 dim^2, inverse update dim (9 dim + 1), normalisation
+    dim^2; x+ and y- steps are forward, x- and y+ inverse."""
+    f_col = 1.5 * P * (P + 1) + 1.5 * Q * (Q + 1) + P + Q + 2
+    f_fwd, f_inv, f_norm = 4 * dim * dim, dim * (9 * dim + 1), dim * dim
+    d = records["dir"][:, :P + Q].astype(np.int64)
+    fwd = np.where(d[:, :P] > 0, d[:, :P], 0).sum(1) + np.where(d[:, P:] < 0, -d[:, P:], 0).sum(1)
+    inv = np.where(d[:, :P] < 0, -d[:, :P], 0).sum(1) + np.where(d[:, P:] > 0, d[:, P:], 0).sum(1)
+    per = N * (fwd * (f_col + f_norm + f_fwd) + inv * (f_col + f_norm + f_inv))
+    return float(per[valid].sum())
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the walk kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "walk_f64_6F5_zeta_delta.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f).get("dram_bytes_per_launch")
+
+
+def cpu_reference(records, threads, budget_s=8.0, max_passes=20):
+    """Time the reference f64 kernel bodies (host build) on the batch."""
+    import oracle
+    kind = "reference" if oracle.have_ref("f64") else "port"
+    run = (lambda: oracle.ref_walk("f64", P, Q, Z, N, H, records, threads=threads)) if kind == "reference" \
+        else (lambda: oracle.walk("f64", P, Q, Z, N, H, records, threads=threads))
+    out = run()  # warm
+    times = []
+    t_all = time.perf_counter()
+    while len(times) < max_passes and (time.perf_counter() - t_all) < budget_s:
+        t0 = time.perf_counter()
+        out = run()
+        times.append(time.perf_counter() - t0)
+    return kind, out, times
+
+
+def verify_counts(desc, records, results, limit_src):
+    from cmfw import exact
+    v = exact.verify(desc, records, results, limit_src, N, H, rtol=RTOL)
+    ok = v["verified"]
+    deltas = results["delta"][ok]
+    deltas = deltas[np.isfinite(deltas)]
+    return int(ok.sum()), v, (float(deltas.max()) if deltas.size else None)
+
+
+def gather_sum(x, world):
+    if world == 1:
+        return [x]
+    import torch.distributed as dist
+    out = [None] * world
+    dist.all_gather_object(out, x)
+    return out
+
+
+def main_cmfw(args):
+    import torch
+    import cmfw
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    records = workload(rank)
+    desc = cmfw.make_desc(P, Q, Z)
+    n = len(records)
+    d_in = cmfw.to_device(records)
+    d_out = cmfw.out_buffer(n)
+    d_src = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step():
+        cmfw.launch_walk(args.variant, desc, d_in, d_out, n, N, H, d_limit_src=d_src)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    time.sleep(0.4)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)  # evict the batch from L2 between steps
+        ev[k][0].record()
+        step()
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_step = float(np.mean(step_ms)) / 1e3
+
+    results = cmfw.records_from_device(d_out, n)
+    src = d_src.cpu().numpy()
+    n_valid = int((results["valid"] == 1).sum())
+    n_ver, vinfo, best_delta = verify_counts(desc, records, results, src)
+    errs = vinfo["rel_err"][vinfo["verified"]]
+
+    # end to end through the host-buffer C ABI, pinned records
+    pin_in = torch.from_numpy(records.view(np.uint8)).pin_memory()
+    pin_out = torch.empty(n * cmfw.OUT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    import ctypes
+    L = cmfw.lib()
+    launch = cmfw._lib.Launch()
+    kms, tms = ctypes.c_float(0), ctypes.c_float(0)
+
+    def e2e_step():
+        cmfw._lib.check(L.cmfw_walk_host(cmfw._lib.VARIANTS[args.variant], ctypes.byref(desc),
+                                         ctypes.c_void_p(pin_in.data_ptr()),
+                                         ctypes.c_void_p(pin_out.data_ptr()), n, N, H, 8,
+                                         ctypes.byref(launch), ctypes.byref(kms), ctypes.byref(tms)))
+
+    e2e_step()
+    e2e_ms = []
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_out = pin_out.numpy().view(cmfw.OUT_DTYPE)
+    assert (e2e_out["valid"] == results["valid"]).all()
+    t_e2e = float(np.mean(e2e_ms)) / 1e3
+
+    # roofline: FP64 pipe
+    flops = flops_per_traj(records, results["valid"] == 1, desc.rank)
+    peak_fp64 = cmfw.pipe_peak(0)
+
+    per_rank = gather_sum({"n_ver": n_ver, "t": t_step, "t_e2e": t_e2e, "n_valid": n_valid}, world)
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    total_ver = sum(r["n_ver"] for r in per_rank)
+    t_max = max(r["t"] for r in per_rank)
+    t_e2e_max = max(r["t_e2e"] for r in per_rank)
+    value = total_ver / t_max
+    achieved = flops / t_step / 1e12
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "verified traj/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": args.variant,
+        "data": "synthetic (seeded std::mt19937_64 directions; no dataset)",
+        "config": {"workload": "6F5 zeta delta search: x=1^6, y=2^5, z=1, rank 5, "
+                               "dirs U{0..3}^11 != 0, N=1000, h=50",
+                   "n_traj_per_gpu": n, "seed": SEED, "variant": args.variant,
+                   "l2": "flushed between steps (256 MiB write outside the timed events)",
+                   "verification": f"exact rational walk (RNS, CRT + rational reconstruction), rtol {RTOL}"},
+        "n_traj": n * world,
+        "n_valid": sum(r["n_valid"] for r in per_rank),
+        "n_verified": total_ver,
+        "traj_per_s": n * world / t_max,
+        "max_rel_err_verified": float(errs.max()) if errs.size else None,
+        "exact_primes_max": int(vinfo["K"].max()) if len(vinfo["K"]) else 0,
+        "best_delta": best_delta,
+        "best_delta_per_gpu_s": (best_delta / (t_max * world)) if best_delta is not None else None,
+        "gpu_launches": args.steps,
+        "e2e": {"value": total_ver / t_e2e_max, "unit": "verified traj/s",
+                "h2d_bytes_per_step": n * 192, "d2h_bytes_per_step": n * 56},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
+                     "frac": achieved / peak_fp64 if peak_fp64 else None,
+                     "peak_source": "in-run FP64 FMA probe (cmfw_pipe_peak); MEASURED_PEAKS.json has no FP64 figure",
+                     "flops_per_launch": flops,
+                     "traffic": ncu_traffic()},
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        kind, cpu_out, times = cpu_reference(records, threads)
+        cpu_ver, _, _ = verify_counts(desc, records, cpu_out, src)
+        t_cpu = float(np.mean(times))
+        line["cpu_baseline"] = {"value": cpu_ver / t_cpu, "unit": "verified traj/s", "cores": threads,
+                                "kind": kind,
+                                "sample": f"the full batch ({n} trajectories) x {len(times)} passes, "
+                                          f"{t_cpu * 1e3:.1f} ms per pass"}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    records = workload(0)
+    import oracle
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.have_ref("f64") else "port"
+    run = (lambda: oracle.ref_walk("f64", P, Q, Z, N, H, records, threads=threads)) if kind == "reference" \
+        else (lambda: oracle.walk("f64", P, Q, Z, N, H, records, threads=threads))
+    for _ in range(args.warmup):
+        run()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out = run()
+        times.append(time.perf_counter() - t0)
+    t = float(np.mean(times))
+    n_ver = None
+    try:
+        import torch
+        import cmfw
+        if torch.cuda.is_available():
+            # which ratio each limit came from (metadata for the exact check)
+            desc = cmfw.make_desc(P, Q, Z)
+            _, src = cmfw.walk("f64", desc, records, N, H, with_limit_src=True)
+            n_ver, _, _ = verify_counts(desc, records, out, src)
+    except Exception as e:  # the check needs the GPU; report the timing regardless
+        print(f"verification unavailable: {e}", file=sys.stderr)
+    value = (n_ver / t) if n_ver is not None else None
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "verified traj/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded std::mt19937_64 directions; no dataset)",
+        "config": {"workload": "6F5 zeta delta search: x=1^6, y=2^5, z=1, rank 5, "
+                               "dirs U{0..3}^11 != 0, N=1000, h=50", "n_traj_per_gpu": NTRAJ,
+                   "seed": SEED},
+        "n_traj": NTRAJ, "n_valid": int((out["valid"] == 1).sum()), "n_verified": n_ver,
+        "traj_per_s": NTRAJ / t,
+        "cpu_baseline": {"value": value, "unit": "verified traj/s", "cores": threads, "kind": kind,
+                         "sample": f"the full batch ({NTRAJ} trajectories) per step"},
+        "e2e": {"value": value, "unit": "verified traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        main_reference(a)
+    else:
+        main_cmfw(a)

@@ -109,6 +109,11 @@ typedef struct {
  * products and sums (the reference compiled for a CPU) instead of fused
  * multiply-adds (the reference compiled by nvcc). */
 #define CMFW_F_UNFUSED_COLUMN 0x2
+/* f64 / df64: walk each trajectory in one thread from step 1 to N instead of
+ * the default chunked walk (a short one-thread prefix, then the remaining
+ * steps split over a CTA and multiplied back in order). block_size is the
+ * CTA size of the chunked walk (64 or 128 threads). */
+#define CMFW_F_SEQUENTIAL 0x4
 
 /* ---- descriptors and library state -------------------------------- */
 
@@ -194,6 +199,10 @@ cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cm
 
 /* Device properties line for the programs' stderr banner. */
 cmfw_status cmfw_device_banner(char *buf, size_t size);
+/* Measured FMA throughput of one pipe on the current device, in tera-ops
+ * per second (an FMA counts 2): pipe 0 = FP64, 1 = FP32, 2 = INT32 IMAD.
+ * The roofline denominator for the walk kernels. Synchronises. */
+cmfw_status cmfw_pipe_peak(int pipe, double *tera_ops_per_s);
 /* cudaMemGetInfo of the current device (device-wide, all processes). */
 cmfw_status cmfw_device_meminfo(size_t *free_bytes, size_t *total_bytes);
 

@@ -26,6 +26,7 @@ TRAJ_STATUS = {0: "ok", 1: "singular_lead", 2: "singular_denom", 3: "singular_so
 
 F_DF64_COMPAT = 0x1
 F_UNFUSED_COLUMN = 0x2
+F_SEQUENTIAL = 0x4
 
 VARIANTS = {"f64": 0, "df64": 1, "rns": 2}
 
@@ -34,7 +35,7 @@ EXPORTS = [
     "cmfw_version", "cmfw_last_error", "cmfw_make_desc", "cmfw_check_desc",
     "cmfw_walk_workspace_bytes", "cmfw_walk_f64", "cmfw_walk_df64", "cmfw_walk_rns",
     "cmfw_rns_trace", "cmfw_exact_residues", "cmfw_reference_inputs", "cmfw_mt64_fill",
-    "cmfw_walk_host", "cmfw_device_banner", "cmfw_device_meminfo",
+    "cmfw_walk_host", "cmfw_pipe_peak", "cmfw_device_banner", "cmfw_device_meminfo",
 ]
 
 
@@ -89,6 +90,7 @@ def lib():
         L.cmfw_walk_host.argtypes = [ci, P(Desc), vp, vp, ci, ci, ci, ci, P(Launch),
                                      P(ctypes.c_float), P(ctypes.c_float)]
         L.cmfw_device_banner.argtypes = [ctypes.c_char_p, cs]
+        L.cmfw_pipe_peak.argtypes = [ci, P(ctypes.c_double)]
         L.cmfw_device_meminfo.argtypes = [P(cs), P(cs)]
         _lib = L
     return _lib

@@ -171,6 +171,13 @@ def exact_residues(desc, records, N, h, primes, pairs=None, d_in=None):
     return d_res.cpu().numpy().view(np.uint32), d_ok.cpu().numpy().astype(bool)
 
 
+def pipe_peak(pipe):
+    """Measured FMA throughput (tera-ops/s, FMA = 2) of pipe 0 FP64, 1 FP32, 2 INT32."""
+    v = ctypes.c_double(0)
+    check(lib().cmfw_pipe_peak(int(pipe), ctypes.byref(v)))
+    return v.value
+
+
 def device_banner():
     buf = ctypes.create_string_buffer(512)
     check(lib().cmfw_device_banner(buf, 512))

@@ -130,9 +130,10 @@ def exact_ratios(desc, records, N, h, pairs=None, K0=64, K_max=4096):
     ratios = [None] * n
     K_used = np.zeros(n, dtype=np.int64)
     todo = np.arange(n)
-    K = K0
-    while len(todo) and K <= K_max:
-        primes = primes_below_2_31(K)
+    K_run = K0
+    while len(todo) and K_run <= K_max:
+        # one GPU run with K_run primes; reconstruction tries growing prefixes
+        primes = primes_below_2_31(K_run)
         sub = records[todo]
         sub_pairs = None if pairs is None else np.asarray(pairs)[todo]
         res, ok = api.exact_residues(desc, sub, N, h, primes.astype(np.uint32), sub_pairs)
@@ -140,21 +141,26 @@ def exact_ratios(desc, records, N, h, pairs=None, K0=64, K_max=4096):
         for li, t in enumerate(todo):
             if not ok[li].any():
                 ratios[t] = None
-                K_used[t] = K
+                K_used[t] = K_run
                 continue
-            rs = []
-            for s in range(3):
-                r = _ratio_from_residues(res[li, s, 0], res[li, s, 1], ok[li], primes)
-                if r is None:
+            K = min(64, K_run)
+            while True:
+                rs = []
+                for s in range(3):
+                    r = _ratio_from_residues(res[li, s, 0, :K], res[li, s, 1, :K], ok[li, :K], primes[:K])
+                    if r is None:
+                        break
+                    rs.append(r)
+                if len(rs) == 3 or K >= K_run:
                     break
-                rs.append(r)
+                K = min(K * 2, K_run)
             if len(rs) < 3:
                 retry.append(t)
             else:
                 ratios[t] = rs
                 K_used[t] = K
         todo = np.array(retry, dtype=np.int64)
-        K *= 4
+        K_run *= 4
     for t in todo:
         K_used[t] = -1  # not determined within K_max primes
     return ratios, K_used
@@ -172,7 +178,7 @@ def exact_estimator(rs, method):
     return r3
 
 
-def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=64):
+def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=1024):
     """Per-trajectory exact check of float results.
 
     Returns a dict of arrays: verified (bool), rel_err (float, nan where not

@@ -1,0 +1,78 @@
+"""Seeded synthetic workloads with the shapes and value ranges of the
+benchmark configurations (the reference's published benchmark inputs are
+reproduced separately by cmfw.reference_inputs).
+
+All draws come from std::mt19937_64 (cmfw.mt64) so C++ and Python callers
+produce identical records; a draw of "uniform in lo..hi" is
+lo + (next() % (hi - lo + 1)).
+"""
+import numpy as np
+
+from . import api
+from ._lib import IN_DTYPE
+
+
+class _Stream:
+    def __init__(self, seed, chunk=1 << 16):
+        self.seed, self.chunk = seed, chunk
+        self.buf = api.mt64(seed, chunk)
+        self.pos = 0
+        self.blocks = 1
+
+    def take(self, n):
+        out = []
+        while n > 0:
+            if self.pos >= len(self.buf):
+                # continue the same std::mt19937_64 sequence
+                self.buf = api.mt64(self.seed, self.chunk * (self.blocks + 1))[self.chunk * self.blocks:]
+                self.blocks += 1
+                self.pos = 0
+            k = min(n, len(self.buf) - self.pos)
+            out.append(self.buf[self.pos:self.pos + k])
+            self.pos += k
+            n -= k
+        return np.concatenate(out) if out else np.zeros(0, dtype=np.uint64)
+
+
+def zeta_start(p, q):
+    """(1, ..., 1; 2, ..., 2), cmf_pfq.cuh:73-79."""
+    return [1.0] * p + [2.0] * q
+
+
+def limit_starts(p, q, n, seed, lo=1, hi=10):
+    """Starts with every coordinate uniform in lo..hi, direction all ones."""
+    s = _Stream(seed)
+    recs = np.zeros(n, dtype=IN_DTYPE)
+    draws = s.take(n * (p + q)).reshape(n, p + q)
+    recs["start"][:, :p + q] = lo + (draws % np.uint64(hi - lo + 1)).astype(np.float64)
+    recs["dir"][:, :p + q] = 1
+    return recs
+
+
+def zeta_directions(p, q, n, seed, lo=0, hi=3, offset=0):
+    """Zeta start; direction components uniform in lo..hi (+ offset),
+    redrawn while all are zero."""
+    s = _Stream(seed)
+    recs = np.zeros(n, dtype=IN_DTYPE)
+    naxes = p + q
+    recs["start"][:, :naxes] = zeta_start(p, q)
+    span = np.uint64(hi - lo + 1)
+    for i in range(n):
+        while True:
+            d = lo + (s.take(naxes) % span).astype(np.int64) + offset
+            if d.any():
+                break
+        recs["dir"][i, :naxes] = d
+    return recs
+
+
+def config(name, seed=20261203):
+    """Records and walk parameters of a named benchmark configuration."""
+    if name == "cfg1":   # 3F2 f64 limit, z = 1/2, starts U{1..10}, dir 1^5
+        return dict(p=3, q=2, z=0.5, N=1000, h=50, records=limit_starts(3, 2, 10000, seed))
+    if name == "cfg2":   # 6F5 zeta delta search, dirs U{0..3}^11 != 0
+        return dict(p=6, q=5, z=1.0, N=1000, h=50, records=zeta_directions(6, 5, 10000, seed))
+    if name == "cfg3":   # 8F7 zeta limit, dir 1^15 + U{0..2}^15
+        return dict(p=8, q=7, z=1.0, N=1000, h=50,
+                    records=zeta_directions(8, 7, 10000, seed, lo=0, hi=2, offset=1))
+    raise ValueError(name)

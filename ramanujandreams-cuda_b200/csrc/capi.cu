@@ -14,8 +14,10 @@
 #include "cmfw_internal.cuh"
 
 namespace cmfw {
-cudaError_t launch_walk_f64(const WalkArgs &W, int block, cudaStream_t s);
-cudaError_t launch_walk_ff(const WalkArgs &W, int block, cudaStream_t s);
+cudaError_t launch_walk_seq(const WalkArgs &W, bool ff, int block, cudaStream_t s);
+cudaError_t launch_walk_chunked(const WalkArgs &W, bool ff, int threads, void *scratch, int prefix_steps,
+                                cudaStream_t s);
+size_t chunk_scratch_bytes(int dim, int n);
 cudaError_t launch_walk_df64_compat(const WalkArgs &W, int block, cudaStream_t s);
 cudaError_t launch_walk_rns(const WalkArgs &W, int n_primes, int trace_steps, uint32_t *trace_res,
                             int *trace_ok, int block, cudaStream_t s);
@@ -95,8 +97,52 @@ cmfw_status ensure_compat_table() {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Device copies of cmfw_walk_host's records, one pair per calling thread
+// and device, kept between calls (the call synchronises before returning).
+struct Staging {
+    void *in = nullptr, *out = nullptr;
+    int cap = 0;
+};
+thread_local std::map<int, Staging> t_staging;
+
+cudaError_t host_staging(int n, cmfw_traj_in **in, cmfw_traj_out **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    Staging &s = t_staging[dev];
+    if (s.cap < n) {
+        cudaFree(s.in);
+        cudaFree(s.out);
+        s.in = s.out = nullptr;
+        s.cap = 0;
+        e = cudaMalloc(&s.in, sizeof(cmfw_traj_in) * (size_t)n);
+        if (e == cudaSuccess) e = cudaMalloc(&s.out, sizeof(cmfw_traj_out) * (size_t)n);
+        if (e != cudaSuccess) return e;
+        s.cap = n;
+    }
+    *in = (cmfw_traj_in *)s.in;
+    *out = (cmfw_traj_out *)s.out;
+    return cudaSuccess;
+}
+
+// Snapshot matrices and row exponents of every trajectory, followed by the
+// chunked walk's prefix products, survivor list and counter.
 size_t snapshot_bytes(int dim, int n) {
-    return align256((size_t)n * 3 * dim * dim * sizeof(double)) + align256((size_t)n * 3 * dim * sizeof(int));
+    return align256((size_t)n * 3 * dim * dim * sizeof(double)) + align256((size_t)n * 3 * dim * sizeof(int)) +
+           chunk_scratch_bytes(dim, n);
+}
+
+void *chunk_scratch(const WalkArgs &W) {
+    return (char *)W.snap_e + align256((size_t)W.n_traj * 3 * W.dim * sizeof(int));
+}
+
+// Lattice steps walked one thread per trajectory before the chunked walk
+// takes over the survivors.
+constexpr int kPrefixSteps = 4;
+
+cudaError_t launch_float_walk(const WalkArgs &W, bool ff, int block, cudaStream_t s) {
+    if (W.flags & CMFW_F_SEQUENTIAL) return launch_walk_seq(W, ff, block, s);
+    return launch_walk_chunked(W, ff, block, chunk_scratch(W), kPrefixSteps, s);
 }
 
 cmfw_status check_walk_args(const cmfw_desc *desc, const void *d_in, const void *d_out, int n, int N,
@@ -188,7 +234,7 @@ cmfw_status cmfw_walk_f64(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_
     WalkArgs W;
     cmfw_status st = prepare(desc, d_in, d_out, n, N, h, launch, s, W);
     if (st != CMFW_OK || n == 0) return st;
-    cudaError_t e = launch_walk_f64(W, block_of(launch), s);
+    cudaError_t e = launch_float_walk(W, false, block_of(launch), s);
     return e == cudaSuccess ? CMFW_OK : cuda_err(e, "f64 walk launch");
 }
 
@@ -199,7 +245,7 @@ cmfw_status cmfw_walk_df64(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw
     cmfw_status st = prepare(desc, d_in, d_out, n, N, h, launch, s, W);
     if (st != CMFW_OK || n == 0) return st;
     cudaError_t e = (W.flags & CMFW_F_DF64_COMPAT) ? launch_walk_df64_compat(W, block_of(launch), s)
-                                                   : launch_walk_ff(W, block_of(launch), s);
+                                                   : launch_float_walk(W, true, block_of(launch), s);
     return e == cudaSuccess ? CMFW_OK : cuda_err(e, "df64 walk launch");
 }
 
@@ -347,8 +393,7 @@ cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cm
     cmfw_traj_in *d_in = nullptr;
     cmfw_traj_out *d_out = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaError_t e = cudaMalloc(&d_in, sizeof(cmfw_traj_in) * (size_t)n);
-    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(cmfw_traj_out) * (size_t)n);
+    cudaError_t e = host_staging(n, &d_in, &d_out);
     for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ev[i]);
     if (e != cudaSuccess) {
         st = set_err(CMFW_ENOMEM, "device buffers for %d trajectories: %s", n, cudaGetErrorString(e));
@@ -380,8 +425,6 @@ cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cm
     }
     for (int i = 0; i < 4; ++i)
         if (ev[i]) cudaEventDestroy(ev[i]);
-    cudaFree(d_in);
-    cudaFree(d_out);
     return st;
 }
 

@@ -304,3 +304,17 @@ __device__ __forceinline__ ff ff_from(double x) {
 __device__ __forceinline__ double ff_to(ff x) { return (double)x.hi + (double)x.lo; }
 
 }  // namespace cmfw
+
+namespace cmfw {
+// Threads per block for a walk kernel: the caller's request (0 = 128),
+// rounded down to a whole number of warps and capped by what the kernel
+// was compiled for (its launch bounds), so any --block-size is accepted.
+inline int clamp_block(const void *kernel, int block) {
+    if (block <= 0) block = 128;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess && block > fa.maxThreadsPerBlock)
+        block = fa.maxThreadsPerBlock;
+    block = (block / 32) * 32;
+    return block < 32 ? 32 : block;
+}
+}  // namespace cmfw

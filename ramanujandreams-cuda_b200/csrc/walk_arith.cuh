@@ -1,0 +1,295 @@
+// The floating-point walk step shared by the sequential and the chunked
+// kernels: arithmetic policies (FP64, float-float), one axis step
+// (cmf_pfq.cuh:255-291 with the column of 146-181 and the update of
+// 186-239), one lattice step (cmf_pfq.cuh:305-322), and the matrix helpers
+// for products of partial walks.
+//
+// Representation: a walk matrix is held either with one power-of-two
+// exponent per row (value = m[r][j] * 2^ex[r]; used while stepping, so a row
+// is only ever rescaled by itself) or with one exponent for the whole matrix
+// (used when partial walks are multiplied together).
+#pragma once
+
+#include "cmfw_internal.cuh"
+#include "walk_common.cuh"
+
+namespace cmfw {
+
+struct ArithF64 {
+    typedef double T;
+    static constexpr int WINDOW = 64;  // rescale outside [2^-64, 2^64)
+    __device__ static __forceinline__ T from(double x) { return x; }
+    __device__ static __forceinline__ double to(T x) { return x; }
+    __device__ static __forceinline__ T mul(T a, T b) { return a * b; }
+    __device__ static __forceinline__ T fma(T a, T b, T c) { return __fma_rn(a, b, c); }
+    __device__ static __forceinline__ T neg(T a) { return -a; }
+    __device__ static __forceinline__ int hexp(T a) { return __double2hiint(a) & 0x7ff00000; }
+    __device__ static __forceinline__ T scale(T a, int be) {
+        return a * __hiloint2double((1023 - be) << 20, 0);
+    }
+    __device__ static __forceinline__ bool nonzero(T a) { return a != 0.0; }
+};
+
+// float-float value hi + lo, |lo| <= ulp(hi)/2.
+struct ArithFF {
+    typedef ff T;
+    static constexpr int WINDOW = 16;  // rescale outside [2^-16, 2^16): FP32 range
+    __device__ static __forceinline__ T from(double x) { return ff_from(x); }
+    __device__ static __forceinline__ double to(T x) { return ff_to(x); }
+    // a*b + c: FMA two-product of the high parts plus cross terms, two-sum
+    // with c's high part, one fast renormalisation.
+    __device__ static __forceinline__ T fma(T a, T b, T c) {
+        float p = a.hi * b.hi;
+        float e = __fmaf_rn(a.hi, b.hi, -p);
+        e = __fmaf_rn(a.hi, b.lo, e);
+        e = __fmaf_rn(a.lo, b.hi, e);
+        float s = p + c.hi;
+        float bb = s - p;
+        float err = (p - (s - bb)) + (c.hi - bb);
+        err = err + (e + c.lo);
+        T r;
+        r.hi = s + err;
+        r.lo = err - (r.hi - s);
+        return r;
+    }
+    __device__ static __forceinline__ T mul(T a, T b) {
+        float p = a.hi * b.hi;
+        float e = __fmaf_rn(a.hi, b.hi, -p);
+        e = __fmaf_rn(a.hi, b.lo, e);
+        e = __fmaf_rn(a.lo, b.hi, e);
+        T r;
+        r.hi = p + e;
+        r.lo = e - (r.hi - p);
+        return r;
+    }
+    __device__ static __forceinline__ T neg(T a) { return T{-a.hi, -a.lo}; }
+    // the high part's exponent field rebased to the double bias, so the
+    // rescale logic is shared with ArithF64
+    __device__ static __forceinline__ int hexp(T a) {
+        int f = (__float_as_int(a.hi) >> 23) & 0xff;
+        if (f == 0) return 0;
+        if (f == 0xff) return 0x7ff00000;
+        return (f - 127 + 1023) << 20;
+    }
+    __device__ static __forceinline__ T scale(T a, int be) {
+        float s = __int_as_float((127 - be) << 23);
+        return T{a.hi * s, a.lo * s};
+    }
+    __device__ static __forceinline__ bool nonzero(T a) { return a.hi != 0.0f; }
+};
+
+template <class A, int DIM>
+__device__ __forceinline__ void rescale(typename A::T (&row)[DIM], int &e) {
+    int hm = 0;
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) hm = max(hm, A::hexp(row[j]));
+    if (hm != 0 && hm < 0x7ff00000 &&
+        (hm >= ((1023 + A::WINDOW) << 20) || hm < ((1023 - A::WINDOW) << 20))) {
+        const int be = (hm >> 20) - 1023;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) row[j] = A::scale(row[j], be);
+        e += be;
+    }
+}
+
+template <class A, int DIM>
+__device__ __forceinline__ bool healthy(const typename A::T (&m)[DIM][DIM]) {
+    bool any_nz = false, bad = false;
+#pragma unroll
+    for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) {
+            bad |= A::hexp(m[r][j]) == 0x7ff00000;
+            any_nz |= A::nonzero(m[r][j]);
+        }
+    return any_nz && !bad;
+}
+
+// Per-launch constants of the walk step.
+struct StepConst {
+    int P, Q;
+    double z;
+    bool rank_reduced_lead;    // lead coefficient is 1 - z (dim == p == q + 1)
+    double lead_scale_fixed;   // max(1, |1 - z|)
+};
+
+// One axis step: M <- M (I + C/a) or M (I + C/a)^-1, then the position
+// moves by `up ? +1 : -1` along `axis`. Returns a cmfw_traj_status.
+template <int DIM, int NAX, int PM, int QM, class A>
+__device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], double (&pos)[NAX],
+                                         int axis, bool up, const StepConst &K) {
+    typedef typename A::T T;
+    const int P = K.P, Q = K.Q;
+    const bool is_x = axis < P;
+    const bool inverse = is_x ? !up : up;
+    // evaluation point: x- steps evaluate at x-1, y+ steps at y+1
+    const double dlt = inverse ? (is_x ? -1.0 : 1.0) : 0.0;
+    double pa = 0.0;
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) pa = (a == axis) ? pos[a] : pa;
+    const double denom = up ? pa : pa - 1.0;
+
+    double xv[PM], yv[QM > 0 ? QM : 1];
+#pragma unroll
+    for (int j = 0; j < PM; ++j) xv[j] = (j < P) ? pos[j] + ((j == axis) ? dlt : 0.0) : 0.0;
+#pragma unroll
+    for (int i = 0; i < QM; ++i) yv[i] = (i < Q) ? (pos[P + i] + ((P + i == axis) ? dlt : 0.0)) - 1.0 : 0.0;
+    double d[DIM + 1];
+    column_poly<PM, QM, DIM>(xv, yv, P, Q, K.z, d);
+    const double lead = d[DIM];
+    bool lead_bad = !isfinite(lead);
+    if (!lead_bad && fabs(lead) < 1.0) {
+        double ls = K.lead_scale_fixed;
+        if (!K.rank_reduced_lead) {
+            ls = 1.0;
+#pragma unroll
+            for (int j = 0; j < PM; ++j) if (j < P) ls += fabs(xv[j]);
+#pragma unroll
+            for (int i = 0; i < QM; ++i) if (i < Q) ls += fabs(yv[i]);
+        }
+        lead_bad = fabs(lead) <= 64.0 * CMFW_EPS64 * ls;
+    }
+    if (lead_bad) return CMFW_TRAJ_SINGULAR_LEAD;
+    if (!isfinite(denom) || fabs(denom) <= 64.0 * CMFW_EPS64) return CMFW_TRAJ_SINGULAR_DENOM;
+    const double il = 1.0 / lead;
+    const double inva_d = 1.0 / denom;
+    double cold[DIM];
+    T col[DIM];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) {
+        cold[i] = -d[i] * il;
+        col[i] = A::from(cold[i]);
+    }
+    const T inva = A::from(inva_d);
+
+    if (!inverse) {
+        // out[j] = m[j] + m[j+1]/a, last += (m . col)/a
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+            T dot = A::mul(m[r][0], col[0]);
+#pragma unroll
+            for (int k = 1; k < DIM; ++k) dot = A::fma(m[r][k], col[k], dot);
+#pragma unroll
+            for (int j = 0; j < DIM - 1; ++j) m[r][j] = A::fma(m[r][j + 1], inva, m[r][j]);
+            m[r][DIM - 1] = A::fma(dot, inva, m[r][DIM - 1]);
+        }
+    } else {
+        // back-substitution in t = out[DIM-1] (cmf_pfq.cuh:207-235); beta and
+        // the scalar solve do not depend on the row and are formed in FP64
+        double be_d[DIM];
+        be_d[DIM - 1] = 1.0;
+#pragma unroll
+        for (int j = DIM - 2; j >= 0; --j) be_d[j] = -be_d[j + 1] * inva_d;
+        double db = be_d[0] * cold[0];
+#pragma unroll
+        for (int k = 1; k < DIM; ++k) db = __fma_rn(be_d[k], cold[k], db);
+        const double sd = __fma_rn(db, inva_d, 1.0);
+        const double ss = fmax(1.0, fabs(db * inva_d));
+        if (!isfinite(sd) || fabs(sd) <= 128.0 * CMFW_EPS64 * ss) return CMFW_TRAJ_SINGULAR_SOLVE;
+        const T isd = A::from(1.0 / sd);
+        const T ninva = A::neg(inva);
+        T be[DIM];
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) be[j] = A::from(be_d[j]);
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+            T al[DIM];
+            al[DIM - 1] = A::from(0.0);
+            al[DIM - 2] = m[r][DIM - 2];
+#pragma unroll
+            for (int j = DIM - 3; j >= 0; --j) al[j] = A::fma(al[j + 1], ninva, m[r][j]);
+            T da = A::mul(al[0], col[0]);
+#pragma unroll
+            for (int k = 1; k < DIM - 1; ++k) da = A::fma(al[k], col[k], da);
+            const T tt = A::mul(A::fma(da, ninva, m[r][DIM - 1]), isd);
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) m[r][j] = A::fma(be[j], tt, al[j]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) rescale<A, DIM>(m[r], ex[r]);
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) pos[a] += (a == axis) ? (up ? 1.0 : -1.0) : 0.0;
+    return CMFW_TRAJ_OK;
+}
+
+// One lattice displacement: levels max|dir| .. 1, axes from the highest
+// down (cmf_pfq.cuh:305-322). Returns a cmfw_traj_status.
+template <int DIM, int NAX, int PM, int QM, class A>
+__device__ __forceinline__ int lattice_step(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], double (&pos)[NAX],
+                                            const int (&absd)[NAX], uint32_t neg, int maxabs,
+                                            const StepConst &K) {
+    for (int level = maxabs; level >= 1; --level) {
+        uint32_t mask = level_mask<NAX>(absd, level);
+        while (mask) {
+            const int axis = top_axis(mask);
+            mask &= ~(1u << axis);
+            const int st = axis_step<DIM, NAX, PM, QM, A>(m, ex, pos, axis, !((neg >> axis) & 1u), K);
+            if (st != CMFW_TRAJ_OK) return st;
+        }
+    }
+    return CMFW_TRAJ_OK;
+}
+
+__device__ __forceinline__ StepConst make_step_const(int P, int Q, int DIM, double z) {
+    StepConst K;
+    K.P = P;
+    K.Q = Q;
+    K.z = z;
+    K.rank_reduced_lead = (DIM == P && P == Q + 1);
+    K.lead_scale_fixed = fmax(1.0, fabs(1.0 - z));
+    return K;
+}
+
+// Rows with their own exponents -> one matrix exponent (the largest row
+// exponent among non-zero rows); written as doubles.
+template <int DIM, class A>
+__device__ __forceinline__ int to_matrix_exponent(const typename A::T (&m)[DIM][DIM], const int (&ex)[DIM],
+                                                  double *out /* DIM*DIM */) {
+    int emax = -0x40000000;
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        bool nz = false;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) nz |= A::nonzero(m[r][j]);
+        if (nz) emax = max(emax, ex[r]);
+    }
+    if (emax == -0x40000000) emax = 0;
+#pragma unroll
+    for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) out[r * DIM + j] = scalbn(A::to(m[r][j]), ex[r] - emax);
+    return emax;
+}
+
+// C = A B for DIM x DIM row-major matrices with matrix exponents; C may
+// alias neither input. Returns C's exponent after a power-of-two rescale
+// that brings its largest entry into [1, 2).
+template <int DIM>
+__device__ __forceinline__ int mat_mul_exp(const double *a, int ea, const double *b, int eb, double *c) {
+    double acc[DIM][DIM];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) {
+            double s = a[i * DIM] * b[j];
+#pragma unroll
+            for (int k = 1; k < DIM; ++k) s = __fma_rn(a[i * DIM + k], b[k * DIM + j], s);
+            acc[i][j] = s;
+        }
+    int hm = 0;
+#pragma unroll
+    for (int i = 0; i < DIM; ++i)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) hm = max(hm, __double2hiint(acc[i][j]) & 0x7ff00000);
+    int be = 0;
+    if (hm != 0 && hm < 0x7ff00000) be = (hm >> 20) - 1023;
+    const double s = __hiloint2double((1023 - be) << 20, 0);
+#pragma unroll
+    for (int i = 0; i < DIM; ++i)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) c[i * DIM + j] = acc[i][j] * s;
+    return ea + eb + be;
+}
+
+}  // namespace cmfw

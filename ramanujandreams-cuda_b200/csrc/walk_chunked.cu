@@ -1,0 +1,247 @@
+// Chunked floating-point walk (default f64 / df64 path).
+//
+// A trajectory's walk is a product of N lattice-step matrices that depend
+// only on the position, never on the accumulated product, so it can be cut
+// into chunks walked independently and multiplied back together in order.
+// Two kernels:
+//
+//  1. prefix: one thread per trajectory walks the first S lattice steps
+//     (S = min(prefix_steps, N-2h-1)). Most trajectories that fail, fail
+//     here (zeta starts hit a singular lead coefficient on their first y+
+//     step), and leave after a handful of steps. Survivors store their
+//     prefix product and append their index to a list.
+//  2. chunk: one CTA of T threads per survivor. The remaining steps form
+//     three segments [S+1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the snapshot
+//     depths are segment ends); each thread walks a contiguous run of lattice
+//     steps of one segment with the same registers-only step as the
+//     sequential kernel, the runs of a segment are multiplied in order by a
+//     shared-memory tree, and thread 0 forms the three snapshots
+//     prefix * seg0, * seg1, * seg2 and reduces them.
+//
+// The latency of one trajectory drops from N lattice steps to about
+// (N - S) / T + log2 T matrix products; the total arithmetic is that of the
+// sequential walk plus T - 1 dense rank^3 products.
+#include "walk_arith.cuh"
+
+namespace cmfw {
+
+struct ChunkArgs {
+    WalkArgs w;
+    double *pre;   // n_traj * DIM * DIM prefix products (matrix exponent form)
+    int *pre_e;    // n_traj
+    int *list;     // n_traj survivor indices
+    int *count;    // survivors
+    int prefix_steps;
+};
+
+template <int P_, int Q_, int DIM, class A>
+__global__ void __launch_bounds__(128) walk_prefix_kernel(ChunkArgs C) {
+    typedef typename A::T T;
+    const WalkArgs &W = C.w;
+    constexpr int NAX = (P_ > 0) ? (P_ + Q_) : CMFW_MAX_AXES;
+    constexpr int PM = (P_ > 0) ? P_ : 8;
+    constexpr int QM = (P_ > 0) ? Q_ : 7;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= W.n_traj) return;
+    const int P = (P_ > 0) ? P_ : W.p;
+    const int Q = (P_ > 0) ? Q_ : W.q;
+    const int naxes = P + Q;
+    const cmfw_traj_in &in = W.in[t];
+    int absd[NAX];
+    uint32_t neg;
+    const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
+    if (maxabs < 0) { write_invalid(W, t, CMFW_TRAJ_STEP_CAP); return; }
+    if (W.N <= 0 || W.h <= 0 || W.N - 2 * W.h <= 0) { write_invalid(W, t, CMFW_TRAJ_BAD_DEPTH); return; }
+    double pos[NAX];
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) pos[a] = (a < naxes) ? in.start[a] : 0.0;
+    T m[DIM][DIM];
+    int ex[DIM];
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        ex[r] = 0;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r == j) ? 1.0 : 0.0);
+    }
+    const StepConst K = make_step_const(P, Q, DIM, W.z);
+    const int S = min(C.prefix_steps, W.N - 2 * W.h - 1);
+    for (int step = 1; step <= S; ++step) {
+        int st = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
+        if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
+        if (st != CMFW_TRAJ_OK) { write_invalid(W, t, st); return; }
+    }
+    C.pre_e[t] = to_matrix_exponent<DIM, A>(m, ex, C.pre + (size_t)t * DIM * DIM);
+    C.list[atomicAdd(C.count, 1)] = t;
+}
+
+template <int P_, int Q_, int DIM, class A, int NT>
+__global__ void __launch_bounds__(NT) walk_chunk_kernel(ChunkArgs C) {
+    typedef typename A::T T;
+    const WalkArgs &W = C.w;
+    constexpr int NAX = (P_ > 0) ? (P_ + Q_) : CMFW_MAX_AXES;
+    constexpr int PM = (P_ > 0) ? P_ : 8;
+    constexpr int QM = (P_ > 0) ? Q_ : 7;
+    constexpr int DD = DIM * DIM;
+    extern __shared__ double smem[];          // NT partial products
+    int *sexp = (int *)(smem + NT * DD);      // NT exponents
+    __shared__ int s_fail;
+
+    if ((int)blockIdx.x >= *C.count) return;  // fewer survivors than CTAs
+    const int t = C.list[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int P = (P_ > 0) ? P_ : W.p;
+    const int Q = (P_ > 0) ? Q_ : W.q;
+    const int naxes = P + Q;
+    const cmfw_traj_in &in = W.in[t];
+    int absd[NAX];
+    uint32_t neg;
+    const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
+    if (tid == 0) s_fail = 0;
+
+    // segments of lattice steps and the threads that walk them
+    const int S = min(C.prefix_steps, W.N - 2 * W.h - 1);
+    const int cp1 = W.N - 2 * W.h, cp2 = W.N - W.h;
+    const int L0 = cp1 - S, L1 = W.h, L2 = W.h;
+    const int rest = W.N - S;
+    int T1 = (NT * L1 + rest / 2) / rest;
+    T1 = max(1, min(T1, L1));
+    int T2 = max(1, min(T1, L2));
+    const int T0 = NT - T1 - T2;
+    const int seg = tid < T0 ? 0 : (tid < T0 + T1 ? 1 : 2);
+    const int base = seg == 0 ? 0 : (seg == 1 ? T0 : T0 + T1);
+    const int Tseg = seg == 0 ? T0 : (seg == 1 ? T1 : T2);
+    const int Lseg = seg == 0 ? L0 : (seg == 1 ? L1 : L2);
+    const int first = seg == 0 ? S + 1 : (seg == 1 ? cp1 + 1 : cp2 + 1);
+    const int local = tid - base;
+    const int lo = first + (int)(((long long)local * Lseg) / Tseg);
+    const int hi = first + (int)(((long long)(local + 1) * Lseg) / Tseg);
+
+    double pos[NAX];
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) {
+        const double d = (a < naxes) ? (double)in.dir[a] : 0.0;
+        pos[a] = (a < naxes) ? in.start[a] + (double)(lo - 1) * d : 0.0;
+    }
+    T m[DIM][DIM];
+    int ex[DIM];
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        ex[r] = 0;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r == j) ? 1.0 : 0.0);
+    }
+    const StepConst K = make_step_const(P, Q, DIM, W.z);
+    __syncthreads();
+    volatile int *fail = &s_fail;
+    for (int step = lo; step < hi; ++step) {
+        if (*fail) break;
+        int st = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
+        if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
+        if (st != CMFW_TRAJ_OK) { *fail = st; break; }
+    }
+    sexp[tid] = to_matrix_exponent<DIM, A>(m, ex, smem + tid * DD);
+    __syncthreads();
+    const int status = s_fail;
+    if (status) {
+        if (tid == 0) write_invalid(W, t, status);
+        return;
+    }
+    // in-order tree product of each segment's runs
+    const int Tmax = max(T0, max(T1, T2));
+    for (int stride = 1; stride < Tmax; stride <<= 1) {
+        if ((local % (2 * stride)) == 0 && local + stride < Tseg)
+            sexp[tid] = mat_mul_exp<DIM>(smem + tid * DD, sexp[tid], smem + (tid + stride) * DD,
+                                         sexp[tid + stride], smem + tid * DD);
+        __syncthreads();
+    }
+    if (tid != 0) return;
+    double *snap = W.snap + (size_t)t * 3 * DD;
+    int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
+    int e = mat_mul_exp<DIM>(C.pre + (size_t)t * DD, C.pre_e[t], smem, sexp[0], snap);
+    int e1 = mat_mul_exp<DIM>(snap, e, smem + T0 * DD, sexp[T0], snap + DD);
+    int e2 = mat_mul_exp<DIM>(snap + DD, e1, smem + (T0 + T1) * DD, sexp[T0 + T1], snap + 2 * DD);
+    const int es[3] = {e, e1, e2};
+    bool ok = true;
+    for (int k = 0; k < 3; ++k) {
+        bool nz = false;
+        for (int i = 0; i < DD; ++i) {
+            const double v = snap[k * DD + i];
+            ok &= isfinite(v);
+            nz |= v != 0.0;
+        }
+        ok &= nz;
+        for (int r = 0; r < DIM; ++r) snap_e[k * DIM + r] = es[k];
+    }
+    if (!ok) { write_invalid(W, t, CMFW_TRAJ_NONFINITE); return; }
+    double ls[3];
+    for (int k = 0; k < 3; ++k) ls[k] = normalise_rows(snap + k * DD, snap_e + k * DIM, DIM, 0.0);
+    finish_valid(W, t, snap, DIM, ls);
+}
+
+typedef void (*chunk_kernel_t)(ChunkArgs);
+
+template <class A, int NT>
+struct ChunkPick {
+    chunk_kernel_t prefix, chunk;
+    int dim;
+};
+
+template <class A, int NT>
+static ChunkPick<A, NT> pick_chunk(int p, int q, int dim) {
+#define CMFW_CASE(P, Q, D)                                                                        \
+    if (p == P && q == Q && dim == D)                                                             \
+        return ChunkPick<A, NT>{walk_prefix_kernel<P, Q, D, A>, walk_chunk_kernel<P, Q, D, A, NT>, D};
+    CMFW_FAMILY_CASES
+#undef CMFW_CASE
+#define CMFW_GEN(D) \
+    case D: return ChunkPick<A, NT>{walk_prefix_kernel<0, 0, D, A>, walk_chunk_kernel<0, 0, D, A, NT>, D};
+    switch (dim) {
+        CMFW_GEN(2) CMFW_GEN(3) CMFW_GEN(4) CMFW_GEN(5) CMFW_GEN(6) CMFW_GEN(7) CMFW_GEN(8)
+    }
+#undef CMFW_GEN
+    return ChunkPick<A, NT>{nullptr, nullptr, 0};
+}
+
+size_t chunk_scratch_bytes(int dim, int n) {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    return al((size_t)n * dim * dim * sizeof(double)) + al((size_t)n * sizeof(int)) * 2 + 256;
+}
+
+template <class A, int NT>
+static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_steps, cudaStream_t s) {
+    ChunkPick<A, NT> k = pick_chunk<A, NT>(W.p, W.q, W.dim);
+    if (!k.prefix) return cudaErrorInvalidValue;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const int dim = W.dim, n = W.n_traj;
+    ChunkArgs C;
+    C.w = W;
+    char *p = (char *)scratch;
+    C.pre = (double *)p;
+    p += al((size_t)n * dim * dim * sizeof(double));
+    C.pre_e = (int *)p;
+    p += al((size_t)n * sizeof(int));
+    C.list = (int *)p;
+    p += al((size_t)n * sizeof(int));
+    C.count = (int *)p;
+    C.prefix_steps = prefix_steps;
+    const size_t shmem = (size_t)NT * dim * dim * sizeof(double) + NT * sizeof(int);
+    cudaError_t e = cudaFuncSetAttribute((const void *)k.chunk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)shmem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(C.count, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    k.prefix<<<(n + 127) / 128, 128, 0, s>>>(C);
+    k.chunk<<<n, NT, shmem, s>>>(C);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk_chunked(const WalkArgs &W, bool ff, int threads, void *scratch, int prefix_steps,
+                                cudaStream_t s) {
+    if (threads > 0 && threads <= 64)
+        return ff ? launch_chunk_t<ArithFF, 64>(W, scratch, prefix_steps, s)
+                  : launch_chunk_t<ArithF64, 64>(W, scratch, prefix_steps, s);
+    return ff ? launch_chunk_t<ArithFF, 128>(W, scratch, prefix_steps, s)
+              : launch_chunk_t<ArithF64, 128>(W, scratch, prefix_steps, s);
+}
+
+}  // namespace cmfw

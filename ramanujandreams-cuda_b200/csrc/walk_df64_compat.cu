@@ -232,7 +232,7 @@ static walk_kernel_t pick_df64_compat(int p, int q, int dim) {
 cudaError_t launch_walk_df64_compat(const WalkArgs &W, int block, cudaStream_t s) {
     walk_kernel_t k = pick_df64_compat(W.p, W.q, W.dim);
     if (!k) return cudaErrorInvalidValue;
-    if (block <= 0) block = 128;
+    block = clamp_block((const void *)k, block);
     k<<<(W.n_traj + block - 1) / block, block, 0, s>>>(W);
     return cudaGetLastError();
 }

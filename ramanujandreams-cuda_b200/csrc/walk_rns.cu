@@ -382,7 +382,7 @@ cudaError_t launch_walk_rns(const WalkArgs &W, int n_primes, int trace_steps, ui
     R.trace_ok = trace_ok;
     rns_kernel_t k = (n_primes > 32) ? pick_rns<2>(W.p, W.q, W.dim) : pick_rns<1>(W.p, W.q, W.dim);
     if (!k) return cudaErrorInvalidValue;
-    if (block <= 0) block = 128;
+    block = clamp_block((const void *)k, block);
     const long long threads = (long long)W.n_traj * L;
     k<<<(unsigned)((threads + block - 1) / block), block, 0, s>>>(R);
     return cudaGetLastError();
