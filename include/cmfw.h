@@ -185,6 +185,9 @@ cmfw_status cmfw_exact_residues(const cmfw_desc *desc, const cmfw_traj_in *d_in,
 cmfw_status cmfw_reference_inputs(int p, int q, int n_traj, int mode, int use_zeta, cmfw_traj_in *h_out);
 /* n outputs of std::mt19937_64(seed), for seeded workload generators. */
 void cmfw_mt64_fill(uint64_t seed, uint64_t *out, size_t n);
+/* Outputs offset .. offset+n-1 of std::mt19937_64(seed): long seeded streams
+ * drawn in pieces without regenerating their start. */
+void cmfw_mt64_fill_at(uint64_t seed, uint64_t offset, uint64_t *out, size_t n);
 
 /* ---- host-buffer convenience (what the drop-in programs call) ------- */
 

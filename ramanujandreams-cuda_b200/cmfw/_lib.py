@@ -35,7 +35,7 @@ EXPORTS = [
     "cmfw_version", "cmfw_last_error", "cmfw_make_desc", "cmfw_check_desc",
     "cmfw_walk_workspace_bytes", "cmfw_walk_f64", "cmfw_walk_df64", "cmfw_walk_rns",
     "cmfw_rns_trace", "cmfw_exact_residues", "cmfw_reference_inputs", "cmfw_mt64_fill",
-    "cmfw_walk_host", "cmfw_pipe_peak", "cmfw_device_banner", "cmfw_device_meminfo",
+    "cmfw_mt64_fill_at", "cmfw_walk_host", "cmfw_pipe_peak", "cmfw_device_banner", "cmfw_device_meminfo",
 ]
 
 
@@ -87,6 +87,8 @@ def lib():
         L.cmfw_reference_inputs.argtypes = [ci, ci, ci, ci, ci, vp]
         L.cmfw_mt64_fill.argtypes = [ctypes.c_uint64, vp, cs]
         L.cmfw_mt64_fill.restype = None
+        L.cmfw_mt64_fill_at.argtypes = [ctypes.c_uint64, ctypes.c_uint64, vp, cs]
+        L.cmfw_mt64_fill_at.restype = None
         L.cmfw_walk_host.argtypes = [ci, P(Desc), vp, vp, ci, ci, ci, ci, P(Launch),
                                      P(ctypes.c_float), P(ctypes.c_float)]
         L.cmfw_device_banner.argtypes = [ctypes.c_char_p, cs]

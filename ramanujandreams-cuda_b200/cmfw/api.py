@@ -33,10 +33,11 @@ def reference_inputs(p, q, n, mode, use_zeta):
     return out
 
 
-def mt64(seed, n):
-    """n outputs of std::mt19937_64(seed)."""
+def mt64(seed, n, offset=0):
+    """Outputs offset .. offset+n-1 of std::mt19937_64(seed)."""
     out = np.zeros(n, dtype=np.uint64)
-    lib().cmfw_mt64_fill(ctypes.c_uint64(seed), out.ctypes.data_as(ctypes.c_void_p), n)
+    lib().cmfw_mt64_fill_at(ctypes.c_uint64(seed), ctypes.c_uint64(offset),
+                            out.ctypes.data_as(ctypes.c_void_p), n)
     return out
 
 

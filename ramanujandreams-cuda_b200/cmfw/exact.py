@@ -209,3 +209,32 @@ def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=1024):
             rel[t] = float(err)
             verified[t] = rel[t] <= rtol
     return {"verified": verified, "rel_err": rel, "exact_limit": exact_limit, "K": Ks}
+
+
+def export_topk(desc, records, results, N, h, k=100, K0=1024):
+    """Exact rational export of the k valid trajectories with the largest
+    finite delta: for each, the ratio p/q = M[0][r-1] / M[1][r-1] at depths
+    N-2h, N-h and N as exact rationals (numerator and denominator as decimal
+    strings), beside the floating-point limit and delta -- the input an exact
+    refinement of the most promising candidates starts from."""
+    delta = np.asarray(results["delta"], float)
+    ok = (np.asarray(results["valid"]) == 1) & np.isfinite(delta)
+    idx = np.nonzero(ok)[0]
+    idx = idx[np.argsort(-delta[idx], kind="stable")][:k]
+    entries = []
+    if len(idx) == 0:
+        return entries
+    ratios, K_used = exact_ratios(desc, records[idx], N, h, K0=K0)
+    p, q = desc.p, desc.q
+    for li, t in enumerate(idx):
+        rs = ratios[li]
+        e = {"index": int(t), "dir": [int(x) for x in records["dir"][t][:p + q]],
+             "start": [float(x) for x in records["start"][t][:p + q]],
+             "delta": float(delta[t]), "limit": float(results["limit"][t]), "primes": int(K_used[li])}
+        if rs is None:
+            e["exact"] = None
+        else:
+            e["exact"] = [None if r == "inf" else {"depth": d, "num": str(r.numerator), "den": str(r.denominator)}
+                          for r, d in zip(rs, (N - 2 * h, N - h, N))]
+        entries.append(e)
+    return entries

@@ -13,23 +13,24 @@ from ._lib import IN_DTYPE
 
 
 class _Stream:
+    """Sequential draws from one std::mt19937_64(seed) stream."""
+
     def __init__(self, seed, chunk=1 << 16):
         self.seed, self.chunk = seed, chunk
-        self.buf = api.mt64(seed, chunk)
+        self.offset = 0  # draws consumed so far
+        self.buf = np.zeros(0, dtype=np.uint64)
         self.pos = 0
-        self.blocks = 1
 
     def take(self, n):
         out = []
         while n > 0:
             if self.pos >= len(self.buf):
-                # continue the same std::mt19937_64 sequence
-                self.buf = api.mt64(self.seed, self.chunk * (self.blocks + 1))[self.chunk * self.blocks:]
-                self.blocks += 1
+                self.buf = api.mt64(self.seed, self.chunk, offset=self.offset)
                 self.pos = 0
             k = min(n, len(self.buf) - self.pos)
             out.append(self.buf[self.pos:self.pos + k])
             self.pos += k
+            self.offset += k
             n -= k
         return np.concatenate(out) if out else np.zeros(0, dtype=np.uint64)
 
@@ -66,6 +67,34 @@ def zeta_directions(p, q, n, seed, lo=0, hi=3, offset=0):
     return recs
 
 
+def valid_directions(p, q, n, seed, z=1.0, N=1000, h=50, lo=0, hi=3, offset=0, batch=1 << 16,
+                     max_draws=1 << 26):
+    """Non-degenerate variant of a zeta direction search: directions drawn as
+    in zeta_directions from one seeded stream, kept only when the f64 walk at
+    (z, N, h) stays valid, until n are kept (seeded rejection sampling; the
+    validity test is the GPU walk, which agrees with the reference's validity
+    trajectory for trajectory)."""
+    s = _Stream(seed)
+    naxes = p + q
+    span = np.uint64(hi - lo + 1)
+    desc = api.make_desc(p, q, z)
+    kept, drawn, have = [], 0, 0
+    while have < n:
+        if drawn >= max_draws:
+            raise RuntimeError(f"only {have} valid directions in {drawn} draws")
+        d = lo + (s.take(batch * naxes) % span).astype(np.int64).reshape(batch, naxes) + offset
+        d = d[d.any(axis=1)]  # all-zero draws are skipped, as in zeta_directions
+        drawn += batch
+        recs = np.zeros(len(d), dtype=IN_DTYPE)
+        recs["start"][:, :naxes] = zeta_start(p, q)
+        recs["dir"][:, :naxes] = d
+        out = api.walk("f64", desc, recs, N, h)
+        good = recs[out["valid"] == 1]
+        kept.append(good)
+        have += len(good)
+    return np.concatenate(kept)[:n]
+
+
 def config(name, seed=20261203):
     """Records and walk parameters of a named benchmark configuration."""
     if name == "cfg1":   # 3F2 f64 limit, z = 1/2, starts U{1..10}, dir 1^5
@@ -75,4 +104,6 @@ def config(name, seed=20261203):
     if name == "cfg3":   # 8F7 zeta limit, dir 1^15 + U{0..2}^15
         return dict(p=8, q=7, z=1.0, N=1000, h=50,
                     records=zeta_directions(8, 7, 10000, seed, lo=0, hi=2, offset=1))
+    if name == "cfg2v":  # cfg2 restricted to directions whose walk stays valid
+        return dict(p=6, q=5, z=1.0, N=1000, h=50, records=valid_directions(6, 5, 2000, seed))
     raise ValueError(name)

@@ -378,6 +378,12 @@ void cmfw_mt64_fill(uint64_t seed, uint64_t *out, size_t n) {
     for (size_t i = 0; i < n; ++i) out[i] = rng();
 }
 
+void cmfw_mt64_fill_at(uint64_t seed, uint64_t offset, uint64_t *out, size_t n) {
+    std::mt19937_64 rng(seed);
+    rng.discard(offset);
+    for (size_t i = 0; i < n; ++i) out[i] = rng();
+}
+
 cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cmfw_traj_in *h_in,
                            cmfw_traj_out *h_out, int n, int N, int h, int n_primes, const cmfw_launch *launch,
                            float *kernel_ms, float *total_ms) {
