@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--impl", default="cmfw", choices=["cmfw", "reference"])
     ap.add_argument("--variant", default="f64", choices=["f64", "df64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="zeta6f5", choices=["zeta6f5", "mixed"],
+                    help="zeta6f5: the headline 6F5 delta search; mixed: the mixed-family batch "
+                         "(10^6 trajectories, N log-uniform 200..5000) in one graph launch")
+    ap.add_argument("--mixed-n", type=int, default=1000000)
     return ap.parse_args()
 
 
@@ -60,6 +64,18 @@ def dist_env():
 def workload(rank):
     import cmfw.workloads as wl
     return wl.zeta_directions(P, Q, NTRAJ, SEED + rank)
+
+
+def walk_flops(p, q, dim, records, Ns, valid):
+    """Algorithmic flops of valid walks (same count as flops_per_traj) for
+    descriptor (p, q, dim) with per-trajectory depths Ns."""
+    f_col = 1.5 * p * (p + 1) + 1.5 * q * (q + 1) + p + q + 2
+    f_fwd, f_inv, f_norm = 4 * dim * dim, dim * (9 * dim + 1), dim * dim
+    d = records["dir"][:, :p + q].astype(np.int64)
+    fwd = np.where(d[:, :p] > 0, d[:, :p], 0).sum(1) + np.where(d[:, p:] < 0, -d[:, p:], 0).sum(1)
+    inv = np.where(d[:, :p] < 0, -d[:, :p], 0).sum(1) + np.where(d[:, p:] > 0, d[:, p:], 0).sum(1)
+    per = np.asarray(Ns, np.float64) * (fwd * (f_col + f_norm + f_fwd) + inv * (f_col + f_norm + f_inv))
+    return float(per[valid].sum())
 
 
 def flops_per_traj(records, valid, dim):
@@ -283,7 +299,7 @@ def main_cmfw(args):
         "exact_primes_max": int(vinfo["K"].max()) if len(vinfo["K"]) else 0,
         "best_delta": best_delta,
         "best_delta_per_gpu_s": (best_delta / (t_max * world)) if best_delta is not None else None,
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps,  # prefix + chunk kernel per step
         "e2e": {"value": total_ver / t_e2e_max, "unit": "verified traj/s",
                 "h2d_bytes_per_step": n * 192, "d2h_bytes_per_step": n * 56},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
@@ -354,9 +370,74 @@ def main_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def main_mixed(args):
+    """Mixed-family batch: 3F2/4F3/5F4/6F5/8F7 x z in {1/2, 1}, starts
+    U{1..10}, directions U{0..3} (not all zero), N log-uniform in 200..5000,
+    h = 50, walked in one CUDA-graph launch (sort + per-descriptor persistent
+    kernels). Reports traj/s of the baseline tiles (one thread per sorted
+    trajectory, 256-thread CTAs), the default tiles and the autotuned tiles."""
+    import torch
+    import cmfw
+    import cmfw.workloads as wl
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    t0 = time.perf_counter()
+    descs, recs, items = wl.mixed_batch(args.mixed_n, SEED)
+    t_gen = time.perf_counter() - t0
+    b = cmfw.MixedBatch(descs, recs, items, H, args.variant)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    t0 = time.perf_counter()
+    tuned = b.autotune()
+    t_tune = time.perf_counter() - t0
+    res = {}
+    for name, tuning in (("baseline_256", cmfw.baseline_tuning()), ("default", None), ("autotuned", tuned)):
+        b.capture(tuning)
+        b.replay()
+        torch.cuda.synchronize()
+        ms = []
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            b.replay()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        out = b.results()
+        res[name] = {"ms": float(np.mean(ms)), "traj_per_s": args.mixed_n / (np.mean(ms) / 1e3),
+                     "n_valid": int((out["valid"] == 1).sum())}
+        b.release()
+    valid = out["valid"] == 1
+    flops = 0.0
+    for di, d in enumerate(descs):
+        m = items["desc"] == di
+        flops += walk_flops(d.p, d.q, d.rank, recs[m], items["N"][m], valid[m])
+    tiles = [{"block": tuned.tile[f].block_size, "grab": tuned.tile[f].grab} for f in range(len(descs))]
+    peak = cmfw.pipe_peak(0 if args.variant == "f64" else 1)
+    best = res["autotuned"]
+    line = {
+        "metric": "mixed-batch traj/s on 1 B200 (one graph launch)", "value": best["traj_per_s"],
+        "unit": "traj/s", "n_gpus": 1, "steps": args.steps, "ms_per_step": best["ms"], "higher_is_better": True,
+        "dtype": args.variant, "data": "synthetic (seeded std::mt19937_64)",
+        "config": {"workload": "mixed: {3F2,4F3,5F4,6F5,8F7} x z{1/2,1}, starts U{1..10}, dirs U{0..3}, "
+                               "N log-uniform 200..5000, h=50", "n_traj": args.mixed_n, "seed": SEED,
+                   "l2": "flushed between steps"},
+        "tiles": res, "autotuned_tiles": tiles, "autotune_s": t_tune, "generate_s": t_gen,
+        "speedup_vs_baseline_256": res["baseline_256"]["ms"] / best["ms"],
+        "roofline": {"bound": "fp64" if args.variant == "f64" else "fp32", "achieved": flops / (best["ms"] / 1e3) / 1e12,
+                     "peak": peak, "unit": "TFLOP/s", "frac": flops / (best["ms"] / 1e3) / 1e12 / peak,
+                     "flops_per_launch": flops},
+    }
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         main_reference(a)
+    elif a.workload == "mixed":
+        main_mixed(a)
     else:
         main_cmfw(a)

@@ -53,12 +53,15 @@ typedef enum {
     CMFW_TRAJ_BAD_DEPTH = 5,       /* N <= 0, h <= 0 or N - 2h <= 0 (cmf_pfq.cuh:352) */
     CMFW_TRAJ_STEP_CAP = 6,        /* |dir| beyond CMFW_MAX_DIR_COMPONENT */
     CMFW_TRAJ_MODULUS_ZERO = 7,    /* exact walk: a divisor vanished modulo this prime */
-    CMFW_TRAJ_NOT_INTEGRAL = 8     /* exact walk: a start coordinate is not an integer */
+    CMFW_TRAJ_NOT_INTEGRAL = 8,    /* exact walk: a start coordinate is not an integer */
+    CMFW_TRAJ_BAD_FAMILY = 9       /* mixed batch: descriptor index out of range */
 } cmfw_traj_status;
 
 /* Largest |dir[a]| a trajectory may use; larger components mark the
  * trajectory CMFW_TRAJ_STEP_CAP instead of walking (bounded device loops). */
 #define CMFW_MAX_DIR_COMPONENT 4096
+/* Largest depth N a walk call accepts (CMFW_EINVAL above it). */
+#define CMFW_MAX_DEPTH (1 << 26)
 
 /* CMFDesc (cmf_pfq.cuh:41-47), same field order and layout. */
 typedef struct {
@@ -111,9 +114,15 @@ typedef struct {
 #define CMFW_F_UNFUSED_COLUMN 0x2
 /* f64 / df64: walk each trajectory in one thread from step 1 to N instead of
  * the default chunked walk (a short one-thread prefix, then the remaining
- * steps split over a CTA and multiplied back in order). block_size is the
- * CTA size of the chunked walk (64 or 128 threads). */
+ * steps split over one CTA per trajectory -- 256 threads up to rank 6, else
+ * 128 -- and multiplied back in order).
+ * block_size is the CTA size of the sequential kernels only. */
 #define CMFW_F_SEQUENTIAL 0x4
+/* f64 chunked walk: walk the runs and multiply them in plain FP64 instead of
+ * double-double. Fewer instructions, but rounding inside a run can be
+ * amplified when the runs are multiplied back together, so results may be
+ * less accurate than the sequential walk's. */
+#define CMFW_F_PLAIN_RUNS 0x8
 
 /* ---- descriptors and library state -------------------------------- */
 
@@ -175,6 +184,59 @@ cmfw_status cmfw_rns_trace(const cmfw_desc *desc, const cmfw_traj_in *d_in, int 
 cmfw_status cmfw_exact_residues(const cmfw_desc *desc, const cmfw_traj_in *d_in, int n_traj,
                                 int N, int h, const uint32_t *d_primes, int K, const int *d_pairs,
                                 uint32_t *d_res, uint8_t *d_prime_ok, void *stream);
+
+/* ---- mixed batches (no reference counterpart: the reference walks one
+ * family at one depth per program run, cmf_walk_f64.cu:156-305) ---------
+ * Trajectories of up to 16 descriptors (family, z) with per-trajectory
+ * depth N in one enqueue: a device counting sort by (descriptor, cost =
+ * N * sum|dir| descending), then per descriptor a persistent kernel whose
+ * warps take cost-sorted trajectories from a queue; the walk of one
+ * trajectory is the sequential walk (f64, or df64 = float-float on the FP32
+ * pipe with an FP64 snapshot reduction). Results land at each trajectory's
+ * own index; a trajectory whose descriptor index is out of range gets
+ * CMFW_TRAJ_BAD_FAMILY. The caller passes a workspace of
+ * cmfw_mixed_workspace_bytes() in launch->d_workspace (the enqueue allocates
+ * nothing, so it can be captured into a CUDA graph); launch->d_status and
+ * d_limit_src work as for the plain walks, block_size is not used. */
+#define CMFW_MAX_MIXED_DESCS 16
+typedef struct {
+    int desc; /* index into the descriptor array */
+    int N;    /* depth; snapshots at N-2h, N-h, N */
+} cmfw_mixed_item;
+typedef struct {
+    int block_size;  /* threads per CTA: 64, 128 or 256 */
+    int grab;        /* trajectories a warp takes per queue access (multiple of 32) */
+    int ctas_per_sm; /* resident CTAs per SM, 0 = as many as fit */
+} cmfw_mixed_tile;
+typedef struct {
+    int persistent; /* 1: cost-sorted queues (tiles below); 0: the baseline, one
+                       thread per sorted trajectory in 256-thread CTAs */
+    cmfw_mixed_tile tile[CMFW_MAX_MIXED_DESCS];
+} cmfw_mixed_tuning;
+size_t cmfw_mixed_workspace_bytes(int n_traj, int n_descs);
+/* tuning NULL = persistent, 128 threads, grab 32, full occupancy. */
+cmfw_status cmfw_walk_mixed(const cmfw_desc *descs, int n_descs, const cmfw_traj_in *d_in,
+                            const cmfw_mixed_item *d_items, cmfw_traj_out *d_out, int n_traj, int h,
+                            int variant, const cmfw_mixed_tuning *tuning, const cmfw_launch *launch,
+                            void *stream);
+/* Autotuner: per descriptor, times every (block 64/128/256) x (grab 32/64)
+ * on a strided sample of up to `sample` (0 = 65536) of that descriptor's
+ * cost-sorted trajectories and keeps the fastest. Synchronises the stream;
+ * writes scratch results into d_out. */
+cmfw_status cmfw_mixed_autotune(const cmfw_desc *descs, int n_descs, const cmfw_traj_in *d_in,
+                                const cmfw_mixed_item *d_items, cmfw_traj_out *d_out, int n_traj, int h,
+                                int variant, const cmfw_launch *launch, int sample, cmfw_mixed_tuning *out,
+                                void *stream);
+/* The whole mixed walk (sort, queues reset, per-descriptor kernels) captured
+ * once into a CUDA graph over fixed buffers and replayed with one launch.
+ * Without launch->d_workspace the graph owns one. */
+typedef struct cmfw_mixed_graph cmfw_mixed_graph;
+cmfw_status cmfw_mixed_graph_create(const cmfw_desc *descs, int n_descs, const cmfw_traj_in *d_in,
+                                    const cmfw_mixed_item *d_items, cmfw_traj_out *d_out, int n_traj, int h,
+                                    int variant, const cmfw_mixed_tuning *tuning, const cmfw_launch *launch,
+                                    cmfw_mixed_graph **out);
+cmfw_status cmfw_mixed_graph_launch(cmfw_mixed_graph *graph, void *stream);
+void cmfw_mixed_graph_destroy(cmfw_mixed_graph *graph);
 
 /* ---- input records -------------------------------------------------- */
 

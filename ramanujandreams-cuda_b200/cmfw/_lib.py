@@ -16,17 +16,20 @@ IN_DTYPE = np.dtype([("dir", "<i4", 16), ("start", "<f8", 16)])
 OUT_DTYPE = np.dtype([("limit", "<f8"), ("delta", "<f8"), ("p", "<f8"), ("q", "<f8"),
                       ("precision", "<f8"), ("log_scale", "<f8"), ("valid", "<i4"),
                       ("n_limits", "<i4")])
+MIXED_ITEM_DTYPE = np.dtype([("desc", "<i4"), ("N", "<i4")])
 assert IN_DTYPE.itemsize == 192 and OUT_DTYPE.itemsize == 56
+MAX_MIXED_DESCS = 16
 
 CMFW_OK = 0
 STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ETIMEOUT", 5: "EUNSUPPORTED"}
 TRAJ_STATUS = {0: "ok", 1: "singular_lead", 2: "singular_denom", 3: "singular_solve",
                4: "nonfinite", 5: "bad_depth", 6: "step_cap", 7: "modulus_zero",
-               8: "not_integral"}
+               8: "not_integral", 9: "bad_family"}
 
 F_DF64_COMPAT = 0x1
 F_UNFUSED_COLUMN = 0x2
 F_SEQUENTIAL = 0x4
+F_PLAIN_RUNS = 0x8
 
 VARIANTS = {"f64": 0, "df64": 1, "rns": 2}
 
@@ -36,6 +39,8 @@ EXPORTS = [
     "cmfw_walk_workspace_bytes", "cmfw_walk_f64", "cmfw_walk_df64", "cmfw_walk_rns",
     "cmfw_rns_trace", "cmfw_exact_residues", "cmfw_reference_inputs", "cmfw_mt64_fill",
     "cmfw_mt64_fill_at", "cmfw_walk_host", "cmfw_pipe_peak", "cmfw_device_banner", "cmfw_device_meminfo",
+    "cmfw_mixed_workspace_bytes", "cmfw_walk_mixed", "cmfw_mixed_autotune", "cmfw_mixed_graph_create",
+    "cmfw_mixed_graph_launch", "cmfw_mixed_graph_destroy",
 ]
 
 
@@ -57,6 +62,16 @@ class Launch(ctypes.Structure):
     _fields_ = [("block_size", ctypes.c_int), ("flags", ctypes.c_int),
                 ("d_status", ctypes.c_void_p), ("d_workspace", ctypes.c_void_p),
                 ("workspace_bytes", ctypes.c_size_t), ("d_limit_src", ctypes.c_void_p)]
+
+
+class MixedTile(ctypes.Structure):
+    """cmfw_mixed_tile: one descriptor's launch shape in a mixed batch."""
+    _fields_ = [("block_size", ctypes.c_int), ("grab", ctypes.c_int), ("ctas_per_sm", ctypes.c_int)]
+
+
+class MixedTuning(ctypes.Structure):
+    """cmfw_mixed_tuning."""
+    _fields_ = [("persistent", ctypes.c_int), ("tile", MixedTile * 16)]
 
 
 _lib = None
@@ -94,6 +109,15 @@ def lib():
         L.cmfw_device_banner.argtypes = [ctypes.c_char_p, cs]
         L.cmfw_pipe_peak.argtypes = [ci, P(ctypes.c_double)]
         L.cmfw_device_meminfo.argtypes = [P(cs), P(cs)]
+        L.cmfw_mixed_workspace_bytes.restype = cs
+        L.cmfw_mixed_workspace_bytes.argtypes = [ci, ci]
+        L.cmfw_walk_mixed.argtypes = [P(Desc), ci, vp, vp, vp, ci, ci, ci, P(MixedTuning), P(Launch), vp]
+        L.cmfw_mixed_autotune.argtypes = [P(Desc), ci, vp, vp, vp, ci, ci, ci, P(Launch), ci, P(MixedTuning), vp]
+        L.cmfw_mixed_graph_create.argtypes = [P(Desc), ci, vp, vp, vp, ci, ci, ci, P(MixedTuning), P(Launch),
+                                              P(vp)]
+        L.cmfw_mixed_graph_launch.argtypes = [vp, vp]
+        L.cmfw_mixed_graph_destroy.argtypes = [vp]
+        L.cmfw_mixed_graph_destroy.restype = None
         _lib = L
     return _lib
 

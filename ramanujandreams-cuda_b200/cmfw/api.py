@@ -9,7 +9,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (IN_DTYPE, OUT_DTYPE, VARIANTS, Desc, Launch, check, lib)
+from ._lib import (IN_DTYPE, MIXED_ITEM_DTYPE, OUT_DTYPE, VARIANTS, Desc, Launch, MixedTuning, check, lib)
 
 
 def make_desc(p, q, z):
@@ -183,3 +183,106 @@ def device_banner():
     buf = ctypes.create_string_buffer(512)
     check(lib().cmfw_device_banner(buf, 512))
     return buf.value.decode()
+
+
+# ---- mixed batches ---------------------------------------------------------
+
+def _descs_array(descs):
+    arr = (Desc * len(descs))()
+    for i, d in enumerate(descs):
+        arr[i] = d
+    return arr
+
+
+def _variant_id(variant):
+    if variant not in ("f64", "df64"):
+        raise ValueError("mixed batches walk in f64 or df64")
+    return VARIANTS[variant]
+
+
+class MixedBatch:
+    """A mixed batch resident on the device: records, per-trajectory
+    (descriptor, depth) items, results and the workspace, ready to walk with
+    cmfw_walk_mixed, to tune with cmfw_mixed_autotune, or to capture once
+    into a CUDA graph (cmfw_mixed_graph_*) and replay."""
+
+    def __init__(self, descs, records, items, h, variant="f64", with_status=False):
+        torch = _torch()
+        self.descs = list(descs)
+        self.c_descs = _descs_array(self.descs)
+        self.n = len(records)
+        self.h = int(h)
+        self.variant = _variant_id(variant)
+        self.d_in = to_device(records)
+        it = np.ascontiguousarray(items, dtype=MIXED_ITEM_DTYPE)
+        self.d_items = torch.from_numpy(it.view(np.int32).reshape(-1)).cuda()
+        self.d_out = out_buffer(self.n)
+        nbytes = lib().cmfw_mixed_workspace_bytes(self.n, len(self.descs))
+        self.d_ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device="cuda")
+        self.d_status = torch.empty(max(self.n, 1), dtype=torch.uint8, device="cuda") if with_status else None
+        self.launch = Launch()
+        self.launch.d_workspace = self.d_ws.data_ptr()
+        self.launch.workspace_bytes = nbytes
+        self.launch.d_status = self.d_status.data_ptr() if with_status else None
+        self._graph = None
+
+    def _args(self):
+        return (self.c_descs, len(self.descs), ctypes.c_void_p(self.d_in.data_ptr()),
+                ctypes.c_void_p(self.d_items.data_ptr()), ctypes.c_void_p(self.d_out.data_ptr()),
+                self.n, self.h, self.variant)
+
+    def walk(self, tuning=None, stream=None):
+        """Enqueue the mixed walk (no synchronisation)."""
+        check(lib().cmfw_walk_mixed(*self._args(), ctypes.byref(tuning) if tuning is not None else None,
+                                    ctypes.byref(self.launch), _stream_handle(stream)))
+
+    def autotune(self, sample=0, stream=None):
+        t = MixedTuning()
+        check(lib().cmfw_mixed_autotune(*self._args(), ctypes.byref(self.launch), int(sample), ctypes.byref(t),
+                                        _stream_handle(stream)))
+        return t
+
+    def capture(self, tuning=None):
+        """Capture the whole walk into a CUDA graph (replaces a previous one)."""
+        self.release()
+        g = ctypes.c_void_p()
+        check(lib().cmfw_mixed_graph_create(*self._args(), ctypes.byref(tuning) if tuning is not None else None,
+                                            ctypes.byref(self.launch), ctypes.byref(g)))
+        self._graph = g
+
+    def replay(self, stream=None):
+        if self._graph is None:
+            raise RuntimeError("capture() first")
+        check(lib().cmfw_mixed_graph_launch(self._graph, _stream_handle(stream)))
+
+    def release(self):
+        if self._graph is not None:
+            lib().cmfw_mixed_graph_destroy(self._graph)
+            self._graph = None
+
+    def results(self):
+        _torch().cuda.synchronize()
+        out = records_from_device(self.d_out, self.n)
+        if self.d_status is not None:
+            return out, self.d_status[:self.n].cpu().numpy()
+        return out
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def baseline_tuning():
+    """The fixed baseline: one thread per sorted trajectory, 256-thread CTAs."""
+    t = MixedTuning()
+    t.persistent = 0
+    return t
+
+
+def walk_mixed(descs, records, items, h, variant="f64", tuning=None, with_status=False):
+    """Walk a mixed batch and return its result records (and statuses)."""
+    b = MixedBatch(descs, records, items, h, variant, with_status)
+    b.walk(tuning)
+    return b.results()

@@ -199,14 +199,18 @@ def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=1024):
             L = exact_estimator(ratios[li], (int(src[t]) >> 12) & 1)
             if L is None:
                 continue
-            Lf = float(L)
-            exact_limit[t] = Lf
+            try:
+                exact_limit[t] = float(L)
+            except OverflowError:  # beyond the double range: no double is within rtol
+                exact_limit[t] = math.inf if L > 0 else -math.inf
             lf = float(results["limit"][t])
-            if Lf == 0.0:
+            if not math.isfinite(lf):
+                err = math.inf
+            elif L == 0:
                 err = abs(lf)
             else:
                 err = abs(Fraction(lf) - L) / abs(L)
-            rel[t] = float(err)
+            rel[t] = float(err) if err < 1e300 else math.inf
             verified[t] = rel[t] <= rtol
     return {"verified": verified, "rel_err": rel, "exact_limit": exact_limit, "K": Ks}
 

@@ -107,3 +107,40 @@ def config(name, seed=20261203):
     if name == "cfg2v":  # cfg2 restricted to directions whose walk stays valid
         return dict(p=6, q=5, z=1.0, N=1000, h=50, records=valid_directions(6, 5, 2000, seed))
     raise ValueError(name)
+
+
+MIXED_FAMILIES = [(3, 2), (4, 3), (5, 4), (6, 5), (8, 7)]
+MIXED_Z = [0.5, 1.0]
+
+
+def mixed_batch(n, seed, N_lo=200, N_hi=5000, lo=1, hi=10, dlo=0, dhi=3):
+    """Mixed batch: CMF family uniform over 3F2, 4F3, 5F4, 6F5, 8F7 and z
+    uniform over {1/2, 1} (descriptor index = 2 * family + z index), start
+    coordinates uniform in lo..hi, direction components uniform in dlo..dhi
+    (redrawn while all are zero), depth N log-uniform in [N_lo, N_hi].
+
+    Returns (descs, records, items) for cmfw.MixedBatch / cmfw.walk_mixed.
+    """
+    from ._lib import MIXED_ITEM_DTYPE
+    descs = [api.make_desc(p, q, z) for (p, q) in MIXED_FAMILIES for z in MIXED_Z]
+    s = _Stream(seed)
+    recs = np.zeros(n, dtype=IN_DTYPE)
+    items = np.zeros(n, dtype=MIXED_ITEM_DTYPE)
+    head = s.take(3 * n).reshape(n, 3)
+    fam = (head[:, 0] % np.uint64(len(MIXED_FAMILIES))).astype(np.int64)
+    zi = (head[:, 1] % np.uint64(len(MIXED_Z))).astype(np.int64)
+    u = (head[:, 2] >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+    items["desc"] = 2 * fam + zi
+    items["N"] = np.floor(N_lo * (N_hi / N_lo) ** u).astype(np.int32)
+    span = np.uint64(hi - lo + 1)
+    dspan = np.uint64(dhi - dlo + 1)
+    for i in range(n):
+        p, q = MIXED_FAMILIES[fam[i]]
+        na = p + q
+        recs["start"][i, :na] = lo + (s.take(na) % span).astype(np.float64)
+        while True:
+            d = dlo + (s.take(na) % dspan).astype(np.int64)
+            if d.any():
+                break
+        recs["dir"][i, :na] = d
+    return descs, recs, items

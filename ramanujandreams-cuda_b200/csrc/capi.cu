@@ -137,8 +137,10 @@ void *chunk_scratch(const WalkArgs &W) {
 }
 
 // Lattice steps walked one thread per trajectory before the chunked walk
-// takes over the survivors.
-constexpr int kPrefixSteps = 4;
+// takes over the survivors: one is enough to drop the walks that fail at
+// once (a singular first step), and the prefix is on every trajectory's
+// critical path.
+constexpr int kPrefixSteps = 1;
 
 cudaError_t launch_float_walk(const WalkArgs &W, bool ff, int block, cudaStream_t s) {
     if (W.flags & CMFW_F_SEQUENTIAL) return launch_walk_seq(W, ff, block, s);
@@ -152,7 +154,7 @@ cmfw_status check_walk_args(const cmfw_desc *desc, const void *d_in, const void 
     if (s != CMFW_OK) return s;
     if (n < 0) return set_err(CMFW_EINVAL, "n_traj = %d is negative", n);
     if (n > 0 && (!d_in || !d_out)) return set_err(CMFW_EINVAL, "NULL trajectory buffer");
-    (void)N;
+    if (N > CMFW_MAX_DEPTH) return set_err(CMFW_EINVAL, "N = %d above CMFW_MAX_DEPTH", N);
     (void)h;
     return CMFW_OK;
 }
@@ -192,6 +194,11 @@ cmfw_status prepare(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_traj_o
 int block_of(const cmfw_launch *launch) { return launch ? launch->block_size : 0; }
 
 }  // namespace
+
+namespace cmfw {
+// cmfw_last_error's message for entry points defined in other files.
+cmfw_status record_error(cmfw_status s, const char *msg) { return set_err(s, "%s", msg); }
+}  // namespace cmfw
 
 extern "C" {
 

@@ -295,6 +295,11 @@ struct ff {
     float hi, lo;
 };
 
+// double-double: hi + lo with |lo| <= ulp(hi)/2
+struct dd {
+    double hi, lo;
+};
+
 __device__ __forceinline__ ff ff_from(double x) {
     ff r;
     r.hi = (float)x;

@@ -8,6 +8,11 @@
 // exponent per row (value = m[r][j] * 2^ex[r]; used while stepping, so a row
 // is only ever rescaled by itself) or with one exponent for the whole matrix
 // (used when partial walks are multiplied together).
+//
+// Error-free transformations (two-sum, two-product) are written with the
+// explicitly rounded intrinsics (__dmul_rn, __dadd_rn, __fmul_rn, ...): the
+// compiler may not contract those into fused multiply-adds, which would
+// break the exactness of the error terms.
 #pragma once
 
 #include "cmfw_internal.cuh"
@@ -15,52 +20,159 @@
 
 namespace cmfw {
 
+struct ArithF64;
+struct ArithDD;
+
 struct ArithF64 {
     typedef double T;
+    typedef ArithF64 Combine;  // arithmetic of the products of partial walks
     static constexpr int WINDOW = 64;  // rescale outside [2^-64, 2^64)
     __device__ static __forceinline__ T from(double x) { return x; }
     __device__ static __forceinline__ double to(T x) { return x; }
     __device__ static __forceinline__ T mul(T a, T b) { return a * b; }
     __device__ static __forceinline__ T fma(T a, T b, T c) { return __fma_rn(a, b, c); }
+    // products with an FP64 scalar of the step matrix (column, 1/a, ...)
+    __device__ static __forceinline__ T fma_s(T a, double s, T c) { return __fma_rn(a, s, c); }
+    __device__ static __forceinline__ T mul_s(T a, double s) { return a * s; }
+    // a / s given inv = 1/s (rounded): the product a*inv refined by one
+    // residual step, q + (a - q s) inv (Markstein), as close to the
+    // correctly rounded quotient as a division
+    __device__ static __forceinline__ T div_s(T a, double s, double inv) {
+        const double q = __dmul_rn(a, inv);
+        return __fma_rn(__fma_rn(-q, s, a), inv, q);
+    }
     __device__ static __forceinline__ T neg(T a) { return -a; }
     __device__ static __forceinline__ int hexp(T a) { return __double2hiint(a) & 0x7ff00000; }
     __device__ static __forceinline__ T scale(T a, int be) {
         return a * __hiloint2double((1023 - be) << 20, 0);
     }
     __device__ static __forceinline__ bool nonzero(T a) { return a != 0.0; }
+    __device__ static __forceinline__ double to_combine(T a) { return a; }
+};
+
+// double-double value hi + lo, |lo| <= ulp(hi)/2 (about 106 significant
+// bits) on the FP64 pipe. The chunked f64 walk computes its partial walks
+// and their products in this arithmetic: a partial walk started from the
+// identity can pass through directions that the true walk state never
+// excites, and rounding those at 53 bits would be amplified when the
+// partial walks are multiplied back together.
+struct ArithDD {
+    typedef dd T;
+    typedef ArithDD Combine;
+    static constexpr int WINDOW = 64;
+    __device__ static __forceinline__ T from(double x) { return T{x, 0.0}; }
+    __device__ static __forceinline__ double to(T x) { return __dadd_rn(x.hi, x.lo); }
+    // a*b + c: FMA two-product of the high parts plus cross terms, two-sum
+    // with c's high part, one fast renormalisation.
+    __device__ static __forceinline__ T fma(T a, T b, T c) {
+        const double p = __dmul_rn(a.hi, b.hi);
+        double e = __fma_rn(a.hi, b.hi, -p);
+        e = __fma_rn(a.hi, b.lo, e);
+        e = __fma_rn(a.lo, b.hi, e);
+        const double s = __dadd_rn(p, c.hi);
+        const double bb = __dsub_rn(s, p);
+        double err = __dadd_rn(__dsub_rn(p, __dsub_rn(s, bb)), __dsub_rn(c.hi, bb));
+        err = __dadd_rn(err, __dadd_rn(e, c.lo));
+        T r;
+        r.hi = __dadd_rn(s, err);
+        r.lo = __dsub_rn(err, __dsub_rn(r.hi, s));
+        return r;
+    }
+    __device__ static __forceinline__ T mul(T a, T b) {
+        const double p = __dmul_rn(a.hi, b.hi);
+        double e = __fma_rn(a.hi, b.hi, -p);
+        e = __fma_rn(a.hi, b.lo, e);
+        e = __fma_rn(a.lo, b.hi, e);
+        T r;
+        r.hi = __dadd_rn(p, e);
+        r.lo = __dsub_rn(e, __dsub_rn(r.hi, p));
+        return r;
+    }
+    // a*s + c and a*s for an FP64 scalar s: one cross term fewer
+    __device__ static __forceinline__ T fma_s(T a, double sc, T c) {
+        const double p = __dmul_rn(a.hi, sc);
+        double e = __fma_rn(a.hi, sc, -p);
+        e = __fma_rn(a.lo, sc, e);
+        const double s = __dadd_rn(p, c.hi);
+        const double bb = __dsub_rn(s, p);
+        double err = __dadd_rn(__dsub_rn(p, __dsub_rn(s, bb)), __dsub_rn(c.hi, bb));
+        err = __dadd_rn(err, __dadd_rn(e, c.lo));
+        T r;
+        r.hi = __dadd_rn(s, err);
+        r.lo = __dsub_rn(err, __dsub_rn(r.hi, s));
+        return r;
+    }
+    __device__ static __forceinline__ T mul_s(T a, double sc) {
+        const double p = __dmul_rn(a.hi, sc);
+        double e = __fma_rn(a.hi, sc, -p);
+        e = __fma_rn(a.lo, sc, e);
+        T r;
+        r.hi = __dadd_rn(p, e);
+        r.lo = __dsub_rn(e, __dsub_rn(r.hi, p));
+        return r;
+    }
+    // a / s to double-double accuracy given inv = 1/s: the leading quotient
+    // digit, the exact remainder a - q1 s, and a second digit from it
+    __device__ static __forceinline__ T div_s(T a, double s, double inv) {
+        const double q1 = __dmul_rn(a.hi, inv);
+        const double p = __dmul_rn(q1, s);
+        const double pe = __fma_rn(q1, s, -p);  // q1 s = p + pe exactly
+        const double r = __dadd_rn(__dsub_rn(__dsub_rn(a.hi, p), pe), a.lo);
+        const double q2 = __dmul_rn(r, inv);
+        T out;
+        out.hi = __dadd_rn(q1, q2);
+        out.lo = __dsub_rn(q2, __dsub_rn(out.hi, q1));
+        return out;
+    }
+    __device__ static __forceinline__ T neg(T a) { return T{-a.hi, -a.lo}; }
+    __device__ static __forceinline__ int hexp(T a) { return __double2hiint(a.hi) & 0x7ff00000; }
+    __device__ static __forceinline__ T scale(T a, int be) {
+        const double s = __hiloint2double((1023 - be) << 20, 0);
+        return T{a.hi * s, a.lo * s};
+    }
+    __device__ static __forceinline__ bool nonzero(T a) { return a.hi != 0.0; }
+    __device__ static __forceinline__ T to_combine(T a) { return a; }
 };
 
 // float-float value hi + lo, |lo| <= ulp(hi)/2.
 struct ArithFF {
     typedef ff T;
+    typedef ArithF64 Combine;
     static constexpr int WINDOW = 16;  // rescale outside [2^-16, 2^16): FP32 range
     __device__ static __forceinline__ T from(double x) { return ff_from(x); }
     __device__ static __forceinline__ double to(T x) { return ff_to(x); }
     // a*b + c: FMA two-product of the high parts plus cross terms, two-sum
     // with c's high part, one fast renormalisation.
     __device__ static __forceinline__ T fma(T a, T b, T c) {
-        float p = a.hi * b.hi;
+        const float p = __fmul_rn(a.hi, b.hi);
         float e = __fmaf_rn(a.hi, b.hi, -p);
         e = __fmaf_rn(a.hi, b.lo, e);
         e = __fmaf_rn(a.lo, b.hi, e);
-        float s = p + c.hi;
-        float bb = s - p;
-        float err = (p - (s - bb)) + (c.hi - bb);
-        err = err + (e + c.lo);
+        const float s = __fadd_rn(p, c.hi);
+        const float bb = __fsub_rn(s, p);
+        float err = __fadd_rn(__fsub_rn(p, __fsub_rn(s, bb)), __fsub_rn(c.hi, bb));
+        err = __fadd_rn(err, __fadd_rn(e, c.lo));
         T r;
-        r.hi = s + err;
-        r.lo = err - (r.hi - s);
+        r.hi = __fadd_rn(s, err);
+        r.lo = __fsub_rn(err, __fsub_rn(r.hi, s));
         return r;
     }
     __device__ static __forceinline__ T mul(T a, T b) {
-        float p = a.hi * b.hi;
+        const float p = __fmul_rn(a.hi, b.hi);
         float e = __fmaf_rn(a.hi, b.hi, -p);
         e = __fmaf_rn(a.hi, b.lo, e);
         e = __fmaf_rn(a.lo, b.hi, e);
         T r;
-        r.hi = p + e;
-        r.lo = e - (r.hi - p);
+        r.hi = __fadd_rn(p, e);
+        r.lo = __fsub_rn(e, __fsub_rn(r.hi, p));
         return r;
+    }
+    // an FP64 scalar enters as its float-float rounding
+    __device__ static __forceinline__ T fma_s(T a, double s, T c) { return fma(a, ff_from(s), c); }
+    __device__ static __forceinline__ T mul_s(T a, double s) { return mul(a, ff_from(s)); }
+    __device__ static __forceinline__ T div_s(T a, double s, double inv) {
+        (void)s;
+        return mul(a, ff_from(inv));
     }
     __device__ static __forceinline__ T neg(T a) { return T{-a.hi, -a.lo}; }
     // the high part's exponent field rebased to the double bias, so the
@@ -76,6 +188,7 @@ struct ArithFF {
         return T{a.hi * s, a.lo * s};
     }
     __device__ static __forceinline__ bool nonzero(T a) { return a.hi != 0.0f; }
+    __device__ static __forceinline__ double to_combine(T a) { return ff_to(a); }
 };
 
 template <class A, int DIM>
@@ -152,58 +265,55 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)
     if (lead_bad) return CMFW_TRAJ_SINGULAR_LEAD;
     if (!isfinite(denom) || fabs(denom) <= 64.0 * CMFW_EPS64) return CMFW_TRAJ_SINGULAR_DENOM;
     const double il = 1.0 / lead;
-    const double inva_d = 1.0 / denom;
-    double cold[DIM];
-    T col[DIM];
+    const double inva = 1.0 / denom;
+    // col = -d / lead: the reciprocal product plus one residual correction
+    // (the reference divides, cmf_pfq.cuh:177)
+    double col[DIM];
 #pragma unroll
     for (int i = 0; i < DIM; ++i) {
-        cold[i] = -d[i] * il;
-        col[i] = A::from(cold[i]);
+        const double c0 = __dmul_rn(-d[i], il);
+        col[i] = __fma_rn(__fma_rn(-c0, lead, -d[i]), il, c0);
     }
-    const T inva = A::from(inva_d);
 
     if (!inverse) {
         // out[j] = m[j] + m[j+1]/a, last += (m . col)/a
 #pragma unroll
         for (int r = 0; r < DIM; ++r) {
-            T dot = A::mul(m[r][0], col[0]);
+            T dot = A::mul_s(m[r][0], col[0]);
 #pragma unroll
-            for (int k = 1; k < DIM; ++k) dot = A::fma(m[r][k], col[k], dot);
+            for (int k = 1; k < DIM; ++k) dot = A::fma_s(m[r][k], col[k], dot);
 #pragma unroll
-            for (int j = 0; j < DIM - 1; ++j) m[r][j] = A::fma(m[r][j + 1], inva, m[r][j]);
-            m[r][DIM - 1] = A::fma(dot, inva, m[r][DIM - 1]);
+            for (int j = 0; j < DIM - 1; ++j) m[r][j] = A::fma_s(m[r][j + 1], inva, m[r][j]);
+            m[r][DIM - 1] = A::fma_s(dot, inva, m[r][DIM - 1]);
         }
     } else {
         // back-substitution in t = out[DIM-1] (cmf_pfq.cuh:207-235); beta and
         // the scalar solve do not depend on the row and are formed in FP64
-        double be_d[DIM];
-        be_d[DIM - 1] = 1.0;
+        double be[DIM];
+        be[DIM - 1] = 1.0;
 #pragma unroll
-        for (int j = DIM - 2; j >= 0; --j) be_d[j] = -be_d[j + 1] * inva_d;
-        double db = be_d[0] * cold[0];
+        for (int j = DIM - 2; j >= 0; --j) be[j] = -be[j + 1] * inva;
+        double db = be[0] * col[0];
 #pragma unroll
-        for (int k = 1; k < DIM; ++k) db = __fma_rn(be_d[k], cold[k], db);
-        const double sd = __fma_rn(db, inva_d, 1.0);
-        const double ss = fmax(1.0, fabs(db * inva_d));
+        for (int k = 1; k < DIM; ++k) db = __fma_rn(be[k], col[k], db);
+        const double sd = __fma_rn(db, inva, 1.0);
+        const double ss = fmax(1.0, fabs(db * inva));
         if (!isfinite(sd) || fabs(sd) <= 128.0 * CMFW_EPS64 * ss) return CMFW_TRAJ_SINGULAR_SOLVE;
-        const T isd = A::from(1.0 / sd);
-        const T ninva = A::neg(inva);
-        T be[DIM];
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) be[j] = A::from(be_d[j]);
+        const double isd = 1.0 / sd;
+        const double ninva = -inva;
 #pragma unroll
         for (int r = 0; r < DIM; ++r) {
             T al[DIM];
             al[DIM - 1] = A::from(0.0);
             al[DIM - 2] = m[r][DIM - 2];
 #pragma unroll
-            for (int j = DIM - 3; j >= 0; --j) al[j] = A::fma(al[j + 1], ninva, m[r][j]);
-            T da = A::mul(al[0], col[0]);
+            for (int j = DIM - 3; j >= 0; --j) al[j] = A::fma_s(al[j + 1], ninva, m[r][j]);
+            T da = A::mul_s(al[0], col[0]);
 #pragma unroll
-            for (int k = 1; k < DIM - 1; ++k) da = A::fma(al[k], col[k], da);
-            const T tt = A::mul(A::fma(da, ninva, m[r][DIM - 1]), isd);
+            for (int k = 1; k < DIM - 1; ++k) da = A::fma_s(al[k], col[k], da);
+            const T tt = A::div_s(A::fma_s(da, ninva, m[r][DIM - 1]), sd, isd);
 #pragma unroll
-            for (int j = 0; j < DIM; ++j) m[r][j] = A::fma(be[j], tt, al[j]);
+            for (int j = 0; j < DIM; ++j) m[r][j] = A::fma_s(tt, be[j], al[j]);
         }
     }
 #pragma unroll
@@ -242,10 +352,11 @@ __device__ __forceinline__ StepConst make_step_const(int P, int Q, int DIM, doub
 }
 
 // Rows with their own exponents -> one matrix exponent (the largest row
-// exponent among non-zero rows); written as doubles.
+// exponent among non-zero rows), written in the combine arithmetic.
 template <int DIM, class A>
 __device__ __forceinline__ int to_matrix_exponent(const typename A::T (&m)[DIM][DIM], const int (&ex)[DIM],
-                                                  double *out /* DIM*DIM */) {
+                                                  typename A::Combine::T *out /* DIM*DIM */) {
+    typedef typename A::Combine C;
     int emax = -0x40000000;
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
@@ -256,39 +367,51 @@ __device__ __forceinline__ int to_matrix_exponent(const typename A::T (&m)[DIM][
     }
     if (emax == -0x40000000) emax = 0;
 #pragma unroll
-    for (int r = 0; r < DIM; ++r)
+    for (int r = 0; r < DIM; ++r) {
+        // rows more than 2^1000 below the largest flush to zero
+        const int be = max(emax - ex[r], 0);
+        const bool keep = be < 1000;
 #pragma unroll
-        for (int j = 0; j < DIM; ++j) out[r * DIM + j] = scalbn(A::to(m[r][j]), ex[r] - emax);
+        for (int j = 0; j < DIM; ++j) {
+            typename C::T v = A::to_combine(m[r][j]);
+            out[r * DIM + j] = keep ? C::scale(v, be) : C::from(0.0);
+        }
+    }
     return emax;
 }
 
-// C = A B for DIM x DIM row-major matrices with matrix exponents; C may
-// alias neither input. Returns C's exponent after a power-of-two rescale
-// that brings its largest entry into [1, 2).
-template <int DIM>
-__device__ __forceinline__ int mat_mul_exp(const double *a, int ea, const double *b, int eb, double *c) {
-    double acc[DIM][DIM];
+// C = A B for DIM x DIM row-major matrices with matrix exponents, in the
+// arithmetic C_ (double or double-double). C may be A itself (each row of C
+// is formed in registers from the same row of A before it is stored) but
+// not B. Returns C's exponent after a power-of-two rescale that brings its
+// largest entry into [1, 2).
+template <int DIM, class C_>
+__device__ __forceinline__ int mat_mul_exp(const typename C_::T *a, int ea, const typename C_::T *b, int eb,
+                                           typename C_::T *c) {
+    typedef typename C_::T T;
+    int hm = 0;
+#pragma unroll 1
+    for (int i = 0; i < DIM; ++i) {
+        T ai[DIM], acc[DIM];
 #pragma unroll
-    for (int i = 0; i < DIM; ++i)
+        for (int k = 0; k < DIM; ++k) ai[k] = a[i * DIM + k];
 #pragma unroll
         for (int j = 0; j < DIM; ++j) {
-            double s = a[i * DIM] * b[j];
+            T s = C_::mul(ai[0], b[j]);
 #pragma unroll
-            for (int k = 1; k < DIM; ++k) s = __fma_rn(a[i * DIM + k], b[k * DIM + j], s);
-            acc[i][j] = s;
+            for (int k = 1; k < DIM; ++k) s = C_::fma(ai[k], b[k * DIM + j], s);
+            acc[j] = s;
+            hm = max(hm, C_::hexp(s));
         }
-    int hm = 0;
 #pragma unroll
-    for (int i = 0; i < DIM; ++i)
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) hm = max(hm, __double2hiint(acc[i][j]) & 0x7ff00000);
+        for (int j = 0; j < DIM; ++j) c[i * DIM + j] = acc[j];
+    }
     int be = 0;
     if (hm != 0 && hm < 0x7ff00000) be = (hm >> 20) - 1023;
-    const double s = __hiloint2double((1023 - be) << 20, 0);
-#pragma unroll
-    for (int i = 0; i < DIM; ++i)
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) c[i * DIM + j] = acc[i][j] * s;
+    if (be != 0) {
+#pragma unroll 1
+        for (int i = 0; i < DIM * DIM; ++i) c[i] = C_::scale(c[i], be);
+    }
     return ea + eb + be;
 }
 

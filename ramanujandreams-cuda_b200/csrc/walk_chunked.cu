@@ -10,8 +10,9 @@
 //     here (zeta starts hit a singular lead coefficient on their first y+
 //     step), and leave after a handful of steps. Survivors store their
 //     prefix product and append their index to a list.
-//  2. chunk: one CTA of T threads per survivor. The remaining steps form
-//     three segments [S+1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the snapshot
+//  2. chunk: one CTA of NT threads (256 up to rank 6, else 128) per
+//     survivor, on a persistent grid (SMs x resident CTAs) that strides
+//     over the survivor list. The remaining steps form three segments [S+1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the snapshot
 //     depths are segment ends); each thread walks a contiguous run of lattice
 //     steps of one segment with the same registers-only step as the
 //     sequential kernel, the runs of a segment are multiplied in order by a
@@ -19,15 +20,30 @@
 //     prefix * seg0, * seg1, * seg2 and reduces them.
 //
 // The latency of one trajectory drops from N lattice steps to about
-// (N - S) / T + log2 T matrix products; the total arithmetic is that of the
-// sequential walk plus T - 1 dense rank^3 products.
+// (N - S) / NT + log2 NT matrix products; the total arithmetic is that of
+// the sequential walk plus NT - 1 dense rank^3 products.
+//
+// Accuracy. Multiplying runs together is a different association of the
+// same matrix product. A run started from the identity can pass through
+// directions that the true walk state never excites (early in a walk, while
+// the positions are still small, the product can grow transiently along
+// them); rounding at that size, once multiplied into the true state, is
+// amplified. The f64 variant therefore walks its runs and multiplies them in
+// double-double (ArithDD, about 106 bits, on the FP64 pipe): rounding inside
+// the runs and the tree then sits far below what the sequential f64 walk
+// commits, and the results keep the sequential walk's accuracy. The
+// per-step matrices themselves (column, 1/a) are formed in FP64 exactly as
+// in the sequential walk. CMFW_F_PLAIN_RUNS selects plain-FP64 runs (fewer
+// instructions, no such guarantee); df64 runs in float-float with FP64
+// products (ArithFF).
 #include "walk_arith.cuh"
 
 namespace cmfw {
 
 struct ChunkArgs {
     WalkArgs w;
-    double *pre;   // n_traj * DIM * DIM prefix products (matrix exponent form)
+    void *pre;     // n_traj * DIM * DIM prefix products (matrix exponent form,
+                   // in the combine arithmetic: double or double-double)
     int *pre_e;    // n_traj
     int *list;     // n_traj survivor indices
     int *count;    // survivors
@@ -70,35 +86,39 @@ __global__ void __launch_bounds__(128) walk_prefix_kernel(ChunkArgs C) {
         if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
         if (st != CMFW_TRAJ_OK) { write_invalid(W, t, st); return; }
     }
-    C.pre_e[t] = to_matrix_exponent<DIM, A>(m, ex, C.pre + (size_t)t * DIM * DIM);
+    typedef typename A::Combine::T CT;
+    C.pre_e[t] = to_matrix_exponent<DIM, A>(m, ex, (CT *)C.pre + (size_t)t * DIM * DIM);
     C.list[atomicAdd(C.count, 1)] = t;
 }
 
-template <int P_, int Q_, int DIM, class A, int NT>
-__global__ void __launch_bounds__(NT) walk_chunk_kernel(ChunkArgs C) {
+// Threads per trajectory: 256 while a thread's registers allow (ranks up to
+// 6), 128 above.
+__host__ __device__ constexpr int chunk_threads(int dim) { return dim <= 6 ? 256 : 128; }
+
+template <int P_, int Q_, int DIM, class A>
+__global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArgs C) {
+    constexpr int NT = chunk_threads(DIM);
     typedef typename A::T T;
+    typedef typename A::Combine CA;
+    typedef typename CA::T CT;
     const WalkArgs &W = C.w;
     constexpr int NAX = (P_ > 0) ? (P_ + Q_) : CMFW_MAX_AXES;
     constexpr int PM = (P_ > 0) ? P_ : 8;
     constexpr int QM = (P_ > 0) ? Q_ : 7;
     constexpr int DD = DIM * DIM;
-    extern __shared__ double smem[];          // NT partial products
-    int *sexp = (int *)(smem + NT * DD);      // NT exponents
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT *smem = (CT *)smem_raw;                  // NT partial products + 3 snapshots
+    int *sexp = (int *)(smem + (NT + 3) * DD);  // NT exponents
+    // earliest failing lattice step of the trajectory, as step * 16 + status
     __shared__ int s_fail;
-
-    if ((int)blockIdx.x >= *C.count) return;  // fewer survivors than CTAs
-    const int t = C.list[blockIdx.x];
     const int tid = threadIdx.x;
     const int P = (P_ > 0) ? P_ : W.p;
     const int Q = (P_ > 0) ? Q_ : W.q;
     const int naxes = P + Q;
-    const cmfw_traj_in &in = W.in[t];
-    int absd[NAX];
-    uint32_t neg;
-    const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
-    if (tid == 0) s_fail = 0;
+    const StepConst K = make_step_const(P, Q, DIM, W.z);
 
-    // segments of lattice steps and the threads that walk them
+    // segments of lattice steps and the threads that walk them (the same
+    // for every trajectory of the launch)
     const int S = min(C.prefix_steps, W.N - 2 * W.h - 1);
     const int cp1 = W.N - 2 * W.h, cp2 = W.N - W.h;
     const int L0 = cp1 - S, L1 = W.h, L2 = W.h;
@@ -115,133 +135,165 @@ __global__ void __launch_bounds__(NT) walk_chunk_kernel(ChunkArgs C) {
     const int local = tid - base;
     const int lo = first + (int)(((long long)local * Lseg) / Tseg);
     const int hi = first + (int)(((long long)(local + 1) * Lseg) / Tseg);
-
-    double pos[NAX];
-#pragma unroll
-    for (int a = 0; a < NAX; ++a) {
-        const double d = (a < naxes) ? (double)in.dir[a] : 0.0;
-        pos[a] = (a < naxes) ? in.start[a] + (double)(lo - 1) * d : 0.0;
-    }
-    T m[DIM][DIM];
-    int ex[DIM];
-#pragma unroll
-    for (int r = 0; r < DIM; ++r) {
-        ex[r] = 0;
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r == j) ? 1.0 : 0.0);
-    }
-    const StepConst K = make_step_const(P, Q, DIM, W.z);
-    __syncthreads();
-    volatile int *fail = &s_fail;
-    for (int step = lo; step < hi; ++step) {
-        if (*fail) break;
-        int st = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
-        if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
-        if (st != CMFW_TRAJ_OK) { *fail = st; break; }
-    }
-    sexp[tid] = to_matrix_exponent<DIM, A>(m, ex, smem + tid * DD);
-    __syncthreads();
-    const int status = s_fail;
-    if (status) {
-        if (tid == 0) write_invalid(W, t, status);
-        return;
-    }
-    // in-order tree product of each segment's runs
     const int Tmax = max(T0, max(T1, T2));
-    for (int stride = 1; stride < Tmax; stride <<= 1) {
-        if ((local % (2 * stride)) == 0 && local + stride < Tseg)
-            sexp[tid] = mat_mul_exp<DIM>(smem + tid * DD, sexp[tid], smem + (tid + stride) * DD,
-                                         sexp[tid + stride], smem + tid * DD);
-        __syncthreads();
-    }
-    if (tid != 0) return;
-    double *snap = W.snap + (size_t)t * 3 * DD;
-    int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
-    int e = mat_mul_exp<DIM>(C.pre + (size_t)t * DD, C.pre_e[t], smem, sexp[0], snap);
-    int e1 = mat_mul_exp<DIM>(snap, e, smem + T0 * DD, sexp[T0], snap + DD);
-    int e2 = mat_mul_exp<DIM>(snap + DD, e1, smem + (T0 + T1) * DD, sexp[T0 + T1], snap + 2 * DD);
-    const int es[3] = {e, e1, e2};
-    bool ok = true;
-    for (int k = 0; k < 3; ++k) {
-        bool nz = false;
-        for (int i = 0; i < DD; ++i) {
-            const double v = snap[k * DD + i];
-            ok &= isfinite(v);
-            nz |= v != 0.0;
+    const int count = *C.count;
+
+    // persistent: CTAs stride over the survivors
+    for (int b = blockIdx.x; b < count; b += gridDim.x) {
+        const int t = C.list[b];
+        const cmfw_traj_in &in = W.in[t];
+        int absd[NAX];
+        uint32_t neg;
+        const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
+        if (tid == 0) s_fail = 0x7fffffff;
+
+        double pos[NAX];
+#pragma unroll
+        for (int a = 0; a < NAX; ++a) {
+            const double d = (a < naxes) ? (double)in.dir[a] : 0.0;
+            pos[a] = (a < naxes) ? in.start[a] + (double)(lo - 1) * d : 0.0;
         }
-        ok &= nz;
-        for (int r = 0; r < DIM; ++r) snap_e[k * DIM + r] = es[k];
+        T m[DIM][DIM];
+        int ex[DIM];
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+            ex[r] = 0;
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r == j) ? 1.0 : 0.0);
+        }
+        __syncthreads();
+        volatile int *fail = &s_fail;
+        for (int step = lo; step < hi; ++step) {
+            if (*fail < step * 16) break;  // an earlier step failed: this run is moot
+            int st = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
+            if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
+            if (st != CMFW_TRAJ_OK) {
+                atomicMin(&s_fail, step * 16 + st);
+                break;
+            }
+        }
+        sexp[tid] = to_matrix_exponent<DIM, A>(m, ex, smem + tid * DD);
+        __syncthreads();
+        const int fkey = s_fail;
+        if (fkey != 0x7fffffff) {
+            if (tid == 0) write_invalid(W, t, fkey & 15);
+            __syncthreads();  // s_fail and the products are reused
+            continue;
+        }
+        // in-order tree product of each segment's runs
+        for (int stride = 1; stride < Tmax; stride <<= 1) {
+            if ((local % (2 * stride)) == 0 && local + stride < Tseg)
+                sexp[tid] = mat_mul_exp<DIM, CA>(smem + tid * DD, sexp[tid], smem + (tid + stride) * DD,
+                                                 sexp[tid + stride], smem + tid * DD);
+            __syncthreads();
+        }
+        if (tid == 0) {
+            // snapshots: prefix * seg0, then * seg1, then * seg2
+            CT *x = smem + NT * DD;
+            const int e = mat_mul_exp<DIM, CA>((const CT *)C.pre + (size_t)t * DD, C.pre_e[t], smem, sexp[0], x);
+            const int e1 = mat_mul_exp<DIM, CA>(x, e, smem + T0 * DD, sexp[T0], x + DD);
+            const int e2 = mat_mul_exp<DIM, CA>(x + DD, e1, smem + (T0 + T1) * DD, sexp[T0 + T1], x + 2 * DD);
+            double *snap = W.snap + (size_t)t * 3 * DD;
+            int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
+            const int es[3] = {e, e1, e2};
+            bool ok = true;
+            for (int k = 0; k < 3; ++k) {
+                bool nz = false;
+                for (int i = 0; i < DD; ++i) {
+                    const double v = CA::to(x[k * DD + i]);
+                    snap[k * DD + i] = v;
+                    ok &= isfinite(v);
+                    nz |= v != 0.0;
+                }
+                ok &= nz;
+                for (int r = 0; r < DIM; ++r) snap_e[k * DIM + r] = es[k];
+            }
+            if (!ok) {
+                write_invalid(W, t, CMFW_TRAJ_NONFINITE);
+            } else {
+                double ls[3];
+                for (int k = 0; k < 3; ++k) ls[k] = normalise_rows(snap + k * DD, snap_e + k * DIM, DIM, 0.0);
+                finish_valid(W, t, snap, DIM, ls);
+            }
+        }
+        __syncthreads();  // shared products are reused by the next trajectory
     }
-    if (!ok) { write_invalid(W, t, CMFW_TRAJ_NONFINITE); return; }
-    double ls[3];
-    for (int k = 0; k < 3; ++k) ls[k] = normalise_rows(snap + k * DD, snap_e + k * DIM, DIM, 0.0);
-    finish_valid(W, t, snap, DIM, ls);
 }
 
 typedef void (*chunk_kernel_t)(ChunkArgs);
 
-template <class A, int NT>
+template <class A>
 struct ChunkPick {
     chunk_kernel_t prefix, chunk;
     int dim;
 };
 
-template <class A, int NT>
-static ChunkPick<A, NT> pick_chunk(int p, int q, int dim) {
+template <class A>
+static ChunkPick<A> pick_chunk(int p, int q, int dim) {
 #define CMFW_CASE(P, Q, D)                                                                        \
     if (p == P && q == Q && dim == D)                                                             \
-        return ChunkPick<A, NT>{walk_prefix_kernel<P, Q, D, A>, walk_chunk_kernel<P, Q, D, A, NT>, D};
+        return ChunkPick<A>{walk_prefix_kernel<P, Q, D, A>, walk_chunk_kernel<P, Q, D, A>, D};
     CMFW_FAMILY_CASES
 #undef CMFW_CASE
 #define CMFW_GEN(D) \
-    case D: return ChunkPick<A, NT>{walk_prefix_kernel<0, 0, D, A>, walk_chunk_kernel<0, 0, D, A, NT>, D};
+    case D: return ChunkPick<A>{walk_prefix_kernel<0, 0, D, A>, walk_chunk_kernel<0, 0, D, A>, D};
     switch (dim) {
         CMFW_GEN(2) CMFW_GEN(3) CMFW_GEN(4) CMFW_GEN(5) CMFW_GEN(6) CMFW_GEN(7) CMFW_GEN(8)
     }
 #undef CMFW_GEN
-    return ChunkPick<A, NT>{nullptr, nullptr, 0};
+    return ChunkPick<A>{nullptr, nullptr, 0};
 }
 
+// Prefix products are stored in the combine arithmetic: at most 16 bytes
+// (double-double) per entry.
 size_t chunk_scratch_bytes(int dim, int n) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    return al((size_t)n * dim * dim * sizeof(double)) + al((size_t)n * sizeof(int)) * 2 + 256;
+    return al((size_t)n * dim * dim * 16) + al((size_t)n * sizeof(int)) * 2 + 256;
 }
 
-template <class A, int NT>
+template <class A>
 static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_steps, cudaStream_t s) {
-    ChunkPick<A, NT> k = pick_chunk<A, NT>(W.p, W.q, W.dim);
+    ChunkPick<A> k = pick_chunk<A>(W.p, W.q, W.dim);
     if (!k.prefix) return cudaErrorInvalidValue;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const int dim = W.dim, n = W.n_traj;
     ChunkArgs C;
     C.w = W;
     char *p = (char *)scratch;
-    C.pre = (double *)p;
-    p += al((size_t)n * dim * dim * sizeof(double));
+    C.pre = (void *)p;
+    p += al((size_t)n * dim * dim * 16);
     C.pre_e = (int *)p;
     p += al((size_t)n * sizeof(int));
     C.list = (int *)p;
     p += al((size_t)n * sizeof(int));
     C.count = (int *)p;
     C.prefix_steps = prefix_steps;
-    const size_t shmem = (size_t)NT * dim * dim * sizeof(double) + NT * sizeof(int);
+    const int NT = chunk_threads(dim);
+    const size_t shmem = (size_t)(NT + 3) * dim * dim * sizeof(typename A::Combine::T) + NT * sizeof(int);
     cudaError_t e = cudaFuncSetAttribute((const void *)k.chunk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shmem);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(C.count, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148, per_sm = 1;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k.chunk, NT, shmem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const int grid = max(1, min(n, sms * per_sm));
     k.prefix<<<(n + 127) / 128, 128, 0, s>>>(C);
-    k.chunk<<<n, NT, shmem, s>>>(C);
+    k.chunk<<<grid, NT, shmem, s>>>(C);
     return cudaGetLastError();
 }
 
+// ff selects the df64 walk (float-float runs); otherwise the f64 walk with
+// double-double runs, or plain FP64 runs with CMFW_F_PLAIN_RUNS.
 cudaError_t launch_walk_chunked(const WalkArgs &W, bool ff, int threads, void *scratch, int prefix_steps,
                                 cudaStream_t s) {
-    if (threads > 0 && threads <= 64)
-        return ff ? launch_chunk_t<ArithFF, 64>(W, scratch, prefix_steps, s)
-                  : launch_chunk_t<ArithF64, 64>(W, scratch, prefix_steps, s);
-    return ff ? launch_chunk_t<ArithFF, 128>(W, scratch, prefix_steps, s)
-              : launch_chunk_t<ArithF64, 128>(W, scratch, prefix_steps, s);
+    (void)threads;
+    if (ff) return launch_chunk_t<ArithFF>(W, scratch, prefix_steps, s);
+    if (W.flags & CMFW_F_PLAIN_RUNS) return launch_chunk_t<ArithF64>(W, scratch, prefix_steps, s);
+    return launch_chunk_t<ArithDD>(W, scratch, prefix_steps, s);
 }
 
 }  // namespace cmfw

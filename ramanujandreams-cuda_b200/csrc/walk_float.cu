@@ -21,70 +21,15 @@
 //  * scalars shared by all rows (column, 1/a, the inverse-step beta vector
 //    and solve) are formed in FP64 for both arithmetics.
 // The singularity tests are the reference's (cmf_pfq.cuh:173, 193, 225).
-#include "walk_arith.cuh"
+#include "walk_seq.cuh"
 
 namespace cmfw {
 
 template <int P_, int Q_, int DIM, class A>
 __global__ void __launch_bounds__(128) walk_float_kernel(WalkArgs W) {
-    typedef typename A::T T;
-    constexpr int NAX = (P_ > 0) ? (P_ + Q_) : CMFW_MAX_AXES;
-    constexpr int PM = (P_ > 0) ? P_ : 8;  // loop bounds for the polynomials
-    constexpr int QM = (P_ > 0) ? Q_ : 7;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= W.n_traj) return;
-    const int P = (P_ > 0) ? P_ : W.p;
-    const int Q = (P_ > 0) ? Q_ : W.q;
-    const int naxes = P + Q;
-    const cmfw_traj_in &in = W.in[t];
-
-    int absd[NAX];
-    uint32_t neg;
-    const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
-    if (maxabs < 0) { write_invalid(W, t, CMFW_TRAJ_STEP_CAP); return; }
-    if (W.N <= 0 || W.h <= 0 || W.N - 2 * W.h <= 0) {
-        write_invalid(W, t, CMFW_TRAJ_BAD_DEPTH);
-        return;
-    }
-    double pos[NAX];
-#pragma unroll
-    for (int a = 0; a < NAX; ++a) pos[a] = (a < naxes) ? in.start[a] : 0.0;
-    T m[DIM][DIM];
-    int ex[DIM];
-#pragma unroll
-    for (int r = 0; r < DIM; ++r) {
-        ex[r] = 0;
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r == j) ? 1.0 : 0.0);
-    }
-    const StepConst K = make_step_const(P, Q, DIM, W.z);
-    const int cp1 = W.N - 2 * W.h, cp2 = W.N - W.h;
-    double *snap = W.snap + (size_t)t * 3 * DIM * DIM;
-    int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
-    int status = CMFW_TRAJ_OK;
-
-    for (int step = 1; step <= W.N; ++step) {
-        status = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
-        if (status != CMFW_TRAJ_OK) break;
-        // The reference fails a step whose matrix is all zero or non-finite
-        // (cmf_pfq.cuh:109); the matrix is checked once per lattice step here.
-        if (!healthy<A, DIM>(m)) { status = CMFW_TRAJ_NONFINITE; break; }
-        const int k = (step == cp1) ? 0 : (step == cp2) ? 1 : (step == W.N) ? 2 : -1;
-        if (k >= 0) {
-#pragma unroll
-            for (int r = 0; r < DIM; ++r) {
-                snap_e[k * DIM + r] = ex[r];
-#pragma unroll
-                for (int j = 0; j < DIM; ++j) snap[(k * DIM + r) * DIM + j] = A::to(m[r][j]);
-            }
-        }
-    }
-    if (status != CMFW_TRAJ_OK) { write_invalid(W, t, status); return; }
-
-    double ls[3];
-#pragma unroll 1
-    for (int k = 0; k < 3; ++k) ls[k] = normalise_rows(snap + k * DIM * DIM, snap_e + k * DIM, DIM, 0.0);
-    finish_valid(W, t, snap, DIM, ls);
+    walk_seq_one<P_, Q_, DIM, A>(W, t, W.N, W.snap + (size_t)t * 3 * DIM * DIM, W.snap_e + (size_t)t * 3 * DIM);
 }
 
 typedef void (*walk_kernel_t)(WalkArgs);
