@@ -145,6 +145,30 @@ size_t cmfw_walk_workspace_bytes(const cmfw_desc *desc, int n_traj);
 cmfw_status cmfw_walk_f64(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_traj_out *d_out,
                           int n_traj, int N, int h, const cmfw_launch *launch, void *stream);
 
+/* ---- f64 walk without any allocation (no counterpart in the reference) --
+ * For callers that cannot call cudaMalloc: code whose device memory all
+ * comes from another allocator's pool (a framework's caching allocator that
+ * must account for every byte), and code that may not synchronise the device
+ * mid-run, which a first cudaMalloc/cudaFree can do. cmfw_walk_f64 without a
+ * caller workspace allocates its scratch on first use; this entry point runs
+ * the same walk (same kernels, same results) with its scratch in a fixed
+ * array of CMFW_NOALLOC_SCRATCH_BYTES inside the library's device image,
+ * which every GPU that loads the library holds until the process exits. The
+ * caller passes device inputs and outputs as for cmfw_walk_f64.
+ *  - Capacity: cmfw_walk_workspace_bytes(desc, n_traj) must not exceed
+ *    CMFW_NOALLOC_SCRATCH_BYTES (about 38,000 trajectories at rank 5, 15,000
+ *    at rank 8); a larger batch returns CMFW_EINVAL, and the caller splits it.
+ *  - Set-up: the first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before capturing any stream.
+ *  - Sharing: all calls on a device share the one array. Calls that overlap
+ *    on the GPU (other streams, other host threads) race on it and give wrong
+ *    results; serialise them on one stream. What must start at zero (the
+ *    survivor counter) is cleared on the stream by each call. */
+#define CMFW_NOALLOC_SCRATCH_BYTES (32u << 20)
+cmfw_status cmfw_walk_f64_noalloc(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_traj_out *d_out,
+                                  int n_traj, int N, int h, void *stream);
+
 /* Replaces walk_kernel_df64<<<...>>>(inputs, results, desc, N, h, n_traj)
  * (cmf_walk_df64.cu:304-306, 410). */
 cmfw_status cmfw_walk_df64(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_traj_out *d_out,

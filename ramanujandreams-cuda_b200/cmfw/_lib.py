@@ -30,13 +30,14 @@ F_DF64_COMPAT = 0x1
 F_UNFUSED_COLUMN = 0x2
 F_SEQUENTIAL = 0x4
 F_PLAIN_RUNS = 0x8
+NOALLOC_SCRATCH_BYTES = 32 << 20  # CMFW_NOALLOC_SCRATCH_BYTES
 
 VARIANTS = {"f64": 0, "df64": 1, "rns": 2}
 
 # Every symbol include/cmfw.h declares.
 EXPORTS = [
     "cmfw_version", "cmfw_last_error", "cmfw_make_desc", "cmfw_check_desc",
-    "cmfw_walk_workspace_bytes", "cmfw_walk_f64", "cmfw_walk_df64", "cmfw_walk_rns",
+    "cmfw_walk_workspace_bytes", "cmfw_walk_f64", "cmfw_walk_f64_noalloc", "cmfw_walk_df64", "cmfw_walk_rns",
     "cmfw_rns_trace", "cmfw_exact_residues", "cmfw_reference_inputs", "cmfw_mt64_fill",
     "cmfw_mt64_fill_at", "cmfw_walk_host", "cmfw_pipe_peak", "cmfw_device_banner", "cmfw_device_meminfo",
     "cmfw_mixed_workspace_bytes", "cmfw_walk_mixed", "cmfw_mixed_autotune", "cmfw_mixed_graph_create",
@@ -96,6 +97,7 @@ def lib():
         L.cmfw_walk_workspace_bytes.argtypes = [P(Desc), ci]
         for name in ("cmfw_walk_f64", "cmfw_walk_df64"):
             getattr(L, name).argtypes = [P(Desc), vp, vp, ci, ci, ci, P(Launch), vp]
+        L.cmfw_walk_f64_noalloc.argtypes = [P(Desc), vp, vp, ci, ci, ci, vp]
         L.cmfw_walk_rns.argtypes = [P(Desc), vp, vp, ci, ci, ci, ci, P(Launch), vp]
         L.cmfw_rns_trace.argtypes = [P(Desc), vp, ci, ci, ci, ci, ci, ci, vp, vp, vp]
         L.cmfw_exact_residues.argtypes = [P(Desc), vp, ci, ci, ci, vp, ci, vp, vp, vp, vp]
