@@ -262,6 +262,54 @@ cmfw_status cmfw_mixed_graph_create(const cmfw_desc *descs, int n_descs, const c
 cmfw_status cmfw_mixed_graph_launch(cmfw_mixed_graph *graph, void *stream);
 void cmfw_mixed_graph_destroy(cmfw_mixed_graph *graph);
 
+/* ---- learned trajectory proposal (no reference counterpart) -----------
+ * A 4-layer MLP (CMFW_MLP_IN -> 256 -> 256 -> 256 -> 1, ReLU) over a
+ * trajectory's features -- direction components dir[0..14] / 4 and a
+ * one-hot of the CMF family (0..4 = 3F2, 4F3, 5F4, 6F5, 8F7) -- that
+ * regresses a walk outcome. Dense layers run as BF16 x BF16 -> FP32
+ * tcgen05 tensor-core GEMMs with fused epilogues; parameters are FP32
+ * masters (BF16 copies for the tensor cores) trained with Adam by the
+ * library's own forward and backward kernels. Batches hold up to the
+ * model's capacity (rounded up to 128). Parameters flatten in the order
+ * W1 [256 x 64], b1, W2 [256 x 256], b2, W3 [256 x 256], b3, w4 [256], b4. */
+#define CMFW_MLP_IN 64
+#define CMFW_MLP_HIDDEN 256
+typedef struct cmfw_mlp cmfw_mlp;
+cmfw_status cmfw_mlp_create(int max_batch, uint64_t seed, cmfw_mlp **out);
+void cmfw_mlp_destroy(cmfw_mlp *mlp);
+size_t cmfw_mlp_param_count(void);
+cmfw_status cmfw_mlp_get_params(cmfw_mlp *mlp, float *h_params);
+cmfw_status cmfw_mlp_set_params(cmfw_mlp *mlp, const float *h_params);
+/* d_score[i] = network(features(d_in[i], d_family[i])). */
+cmfw_status cmfw_mlp_forward(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const int *d_family, int n,
+                             float *d_score, void *stream);
+/* Gradients of loss = sum_i w_i (score_i - target_i)^2 / weight_sum (w = 1
+ * when d_weight is NULL) into h_grads (cmfw_mlp_param_count floats) and the
+ * loss into *h_loss; synchronises. */
+cmfw_status cmfw_mlp_gradients(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const int *d_family,
+                               const float *d_target, const float *d_weight, int n, float weight_sum,
+                               float *h_grads, float *h_loss, void *stream);
+/* One Adam step (beta 0.9 / 0.999) on that loss; *d_loss gets the loss. */
+cmfw_status cmfw_mlp_train_step(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const int *d_family,
+                                const float *d_target, const float *d_weight, int n, float weight_sum,
+                                float lr, float *d_loss, void *stream);
+/* CMFW_ETIMEOUT if a bounded tensor-core wait of an earlier call gave up. */
+cmfw_status cmfw_mlp_status(cmfw_mlp *mlp);
+/* Candidates first .. first+n-1 of a seeded generator: direction component
+ * a of candidate i is lo + (16-bit field of splitmix64 draws) mod
+ * (hi - lo + 1) for the first naxes axes (naxes <= 15). Scores all of them
+ * with the network (family one-hot `family`) into d_scores[0..n). */
+cmfw_status cmfw_mlp_score_candidates(cmfw_mlp *mlp, uint64_t seed, long long first, long long n, int naxes,
+                                      int lo, int hi, int family, float *d_scores, void *stream);
+/* Records of the candidates d_idx[0..n) of the same generator, start d_start. */
+cmfw_status cmfw_candidate_records(uint64_t seed, const long long *d_idx, int n, int naxes, int lo, int hi,
+                                   const double *d_start, cmfw_traj_in *d_out, void *stream);
+/* Indices of the k largest of d_scores[0..n) (ties at the threshold
+ * included, at most cap written) into d_idx, their number in *h_count;
+ * synchronises. */
+cmfw_status cmfw_select_top(const float *d_scores, long long n, long long k, long long *d_idx, int cap,
+                            int *h_count, void *stream);
+
 /* ---- input records -------------------------------------------------- */
 
 /* The reference programs' input records for `mode` (0 = limit, 1 = delta)

@@ -19,6 +19,9 @@ OUT_DTYPE = np.dtype([("limit", "<f8"), ("delta", "<f8"), ("p", "<f8"), ("q", "<
 MIXED_ITEM_DTYPE = np.dtype([("desc", "<i4"), ("N", "<i4")])
 assert IN_DTYPE.itemsize == 192 and OUT_DTYPE.itemsize == 56
 MAX_MIXED_DESCS = 16
+MLP_IN, MLP_HIDDEN = 64, 256
+# flattened parameter shapes: W1, b1, W2, b2, W3, b3, w4, b4
+MLP_SHAPES = [(256, 64), (256,), (256, 256), (256,), (256, 256), (256,), (256,), (1,)]
 
 CMFW_OK = 0
 STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ETIMEOUT", 5: "EUNSUPPORTED"}
@@ -42,6 +45,9 @@ EXPORTS = [
     "cmfw_mt64_fill_at", "cmfw_walk_host", "cmfw_pipe_peak", "cmfw_device_banner", "cmfw_device_meminfo",
     "cmfw_mixed_workspace_bytes", "cmfw_walk_mixed", "cmfw_mixed_autotune", "cmfw_mixed_graph_create",
     "cmfw_mixed_graph_launch", "cmfw_mixed_graph_destroy",
+    "cmfw_mlp_create", "cmfw_mlp_destroy", "cmfw_mlp_param_count", "cmfw_mlp_get_params", "cmfw_mlp_set_params",
+    "cmfw_mlp_forward", "cmfw_mlp_gradients", "cmfw_mlp_train_step", "cmfw_mlp_status",
+    "cmfw_mlp_score_candidates", "cmfw_candidate_records", "cmfw_select_top",
 ]
 
 
@@ -120,6 +126,20 @@ def lib():
         L.cmfw_mixed_graph_launch.argtypes = [vp, vp]
         L.cmfw_mixed_graph_destroy.argtypes = [vp]
         L.cmfw_mixed_graph_destroy.restype = None
+        fp, ll, u64 = ctypes.c_float, ctypes.c_longlong, ctypes.c_uint64
+        L.cmfw_mlp_create.argtypes = [ci, u64, P(vp)]
+        L.cmfw_mlp_destroy.argtypes = [vp]
+        L.cmfw_mlp_destroy.restype = None
+        L.cmfw_mlp_param_count.restype = cs
+        L.cmfw_mlp_get_params.argtypes = [vp, vp]
+        L.cmfw_mlp_set_params.argtypes = [vp, vp]
+        L.cmfw_mlp_forward.argtypes = [vp, vp, vp, ci, vp, vp]
+        L.cmfw_mlp_gradients.argtypes = [vp, vp, vp, vp, vp, ci, fp, vp, vp, vp]
+        L.cmfw_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, ci, fp, fp, vp, vp]
+        L.cmfw_mlp_status.argtypes = [vp]
+        L.cmfw_mlp_score_candidates.argtypes = [vp, u64, ll, ll, ci, ci, ci, ci, vp, vp]
+        L.cmfw_candidate_records.argtypes = [u64, vp, ci, ci, ci, ci, vp, vp, vp]
+        L.cmfw_select_top.argtypes = [vp, ll, ll, vp, ci, P(ci), vp]
         _lib = L
     return _lib
 

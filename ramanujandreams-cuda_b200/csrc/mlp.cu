@@ -1,0 +1,764 @@
+// Learned trajectory proposal: a 4-layer MLP (64 -> 256 -> 256 -> 256 -> 1,
+// ReLU) over a trajectory's direction and CMF family, trained on walk
+// results by this file's kernels and used to rank candidate directions.
+//
+// The three dense layers run on the 5th-generation tensor cores:
+// gemm_bf16_kernel computes C = epilogue(A * B^T) for BF16 K-major operands
+// with tcgen05.mma (M = 128 rows per CTA, N = 64/128/256), the FP32
+// accumulator in tensor memory, operands staged in shared memory through a
+// two-stage cp.async ring in the interleaved canonical layout
+// (tc_sm100.cuh), and the epilogue (bias + ReLU + BF16 rounding, or the
+// ReLU-derivative mask of the backward pass, or FP32 out) fused after the
+// tcgen05.ld of the accumulator. Forward:  Z = X W^T (A = activations,
+// B = W stored [out x in]). Backward: dX = dZ W (B = W^T stored [in x out]),
+// dW = dZ^T X (A = dZ^T, B = X^T, both transposed by transpose_bf16_kernel).
+// The 256 -> 1 head, the loss, bias gradients and Adam are CUDA-core kernels.
+//
+// Inputs: features(t) = (dir[0..14] / 4, one-hot(family) over 5, zeros) as
+// 64 BF16 values. Parameters are FP32 masters with BF16 copies for the
+// tensor cores (W and W^T).
+#include <cstdio>
+#include <cstring>
+#include <cuda_bf16.h>
+#include <vector>
+
+#include "cmfw.h"
+#include "cmfw_internal.cuh"
+#include "tc_sm100.cuh"
+
+namespace cmfw {
+cmfw_status record_error(cmfw_status s, const char *msg);
+
+constexpr int kIn = CMFW_MLP_IN;       // 64
+constexpr int kHid = CMFW_MLP_HIDDEN;  // 256
+constexpr int kBK = 64;                // K per pipeline stage
+
+enum { EPI_BIAS_RELU_BF16 = 0, EPI_F32 = 1, EPI_MASK_BF16 = 2 };
+
+struct GemmArgs {
+    const __nv_bfloat16 *A;  // M x K, row stride lda
+    const __nv_bfloat16 *B;  // N x K, row stride ldb
+    int M, N, K, lda, ldb;
+    void *C;  // M x N, row stride ldc (bf16 or f32)
+    int ldc;
+    const float *bias;           // EPI_BIAS_RELU_BF16: N
+    const __nv_bfloat16 *mask;   // EPI_MASK_BF16: M x N, row stride ldc; C = acc where mask > 0
+    int *err;
+};
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// One 64-wide K chunk of a ROWS x K operand into an interleaved tile.
+template <int ROWS>
+__device__ __forceinline__ void load_chunk(uint32_t tile, const __nv_bfloat16 *src, int ld, int row0, int k0) {
+#pragma unroll
+    for (int i = threadIdx.x; i < ROWS * 8; i += 128) {
+        const int r = i >> 3, c = i & 7;
+        cp_async16(tile + (uint32_t)((r >> 3) * 1024 + c * 128 + (r & 7) * 16),
+                   src + (size_t)(row0 + r) * ld + k0 + c * 8);
+    }
+}
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
+    constexpr int A_BYTES = 128 * kBK * 2;
+    constexpr int B_BYTES = BN * kBK * 2;
+    constexpr int STAGE = A_BYTES + B_BYTES;
+    constexpr uint32_t TCOLS = BN < 32 ? 32 : BN;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_bad;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * 128, n0 = blockIdx.x * BN;
+    const int nk = g.K / kBK;
+    const uint32_t sbase = tc::smem_u32(smem);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        s_bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_base, TCOLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, BN);
+    bool ok = true;
+
+    load_chunk<128>(sbase, g.A, g.lda, m0, 0);
+    load_chunk<BN>(sbase + A_BYTES, g.B, g.ldb, n0, 0);
+    cp_async_commit();
+    for (int kc = 0; kc < nk; ++kc) {
+        const int s = kc & 1;
+        if (kc + 1 < nk) {
+            // the other stage was last read by the MMAs of chunk kc - 1
+            if (kc >= 1 && !tc::mbar_wait(&bar[s ^ 1], ((kc - 1) >> 1) & 1)) ok = false;
+            const uint32_t st = sbase + (uint32_t)((s ^ 1) * STAGE);
+            load_chunk<128>(st, g.A, g.lda, m0, (kc + 1) * kBK);
+            load_chunk<BN>(st + A_BYTES, g.B, g.ldb, n0, (kc + 1) * kBK);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc::fence_after_sync();
+            const uint32_t a = sbase + (uint32_t)(s * STAGE), b = a + A_BYTES;
+#pragma unroll
+            for (int j = 0; j < kBK / 16; ++j)
+                tc::mma_bf16(tmem, tc::smem_desc(a + j * 256, 128, 1024), tc::smem_desc(b + j * 256, 128, 1024),
+                             idesc, kc > 0 || j > 0);
+            tc::commit(&bar[s]);
+        }
+    }
+    if (!tc::mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1)) {
+        ok = false;
+        tc::mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1);  // one more bounded wait before freeing TMEM
+    }
+    if (!ok) s_bad = 1;
+    __syncthreads();
+    tc::fence_after_sync();
+    if (s_bad) {
+        if (threadIdx.x == 0) atomicExch(g.err, 1);
+    } else {
+        const int row = m0 + warp * 32 + lane;
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+            float v[32];
+            tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            const int col = n0 + c0;
+            if (EPI == EPI_F32) {
+                float *dst = (float *)g.C + (size_t)row * g.ldc + col;
+#pragma unroll
+                for (int i = 0; i < 32; i += 4) *(float4 *)(dst + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+            } else {
+                __nv_bfloat16 *dst = (__nv_bfloat16 *)g.C + (size_t)row * g.ldc + col;
+                if (EPI == EPI_BIAS_RELU_BF16) {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) v[i] = fmaxf(v[i] + g.bias[col + i], 0.0f);
+                } else {
+                    const __nv_bfloat16 *mk = g.mask + (size_t)row * g.ldc + col;
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) v[i] = __bfloat162float(mk[i]) > 0.0f ? v[i] : 0.0f;
+                }
+#pragma unroll
+                for (int i = 0; i < 32; i += 8) {
+                    __nv_bfloat162 h[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) h[j] = __floats2bfloat162_rn(v[i + 2 * j], v[i + 2 * j + 1]);
+                    *(uint4 *)(dst + i) = *(uint4 *)h;
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, TCOLS);
+}
+
+template <int BN, int EPI>
+static cudaError_t gemm_launch(const GemmArgs &g, cudaStream_t s) {
+    constexpr int smem = 2 * (128 * kBK * 2 + BN * kBK * 2) + 1024;
+    cudaError_t e = cudaFuncSetAttribute((const void *)gemm_bf16_kernel<BN, EPI>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(g.N / BN, g.M / 128);
+    gemm_bf16_kernel<BN, EPI><<<grid, 128, smem, s>>>(g);
+    return cudaGetLastError();
+}
+
+// Host-side shape rules: M % 128, K % 64, N % 64 == 0; 16-byte aligned rows.
+static cudaError_t gemm(const GemmArgs &g, int epi, cudaStream_t s) {
+    if (g.M % 128 || g.K % kBK || g.N % 64 || g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaErrorInvalidValue;
+    const bool n256 = g.N % 256 == 0;
+    if (epi == EPI_BIAS_RELU_BF16) return n256 ? gemm_launch<256, EPI_BIAS_RELU_BF16>(g, s)
+                                              : gemm_launch<64, EPI_BIAS_RELU_BF16>(g, s);
+    if (epi == EPI_MASK_BF16) return n256 ? gemm_launch<256, EPI_MASK_BF16>(g, s) : gemm_launch<64, EPI_MASK_BF16>(g, s);
+    return n256 ? gemm_launch<256, EPI_F32>(g, s) : gemm_launch<64, EPI_F32>(g, s);
+}
+
+// ---- CUDA-core kernels ------------------------------------------------------
+
+// Features of n trajectories into X [n_pad x 64] bf16 (rows >= n zero).
+__global__ void features_kernel(const cmfw_traj_in *in, const int *family, int n, int n_pad, __nv_bfloat16 *X) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pad * kIn) return;
+    const int t = i / kIn, c = i % kIn;
+    float v = 0.0f;
+    if (t < n) {
+        if (c < 15) v = 0.25f * (float)in[t].dir[c];
+        else if (c < 20) v = (family[t] == c - 15) ? 1.0f : 0.0f;
+    }
+    X[i] = __float2bfloat16_rn(v);
+}
+
+// Candidate directions from a counter-based generator (splitmix64 of
+// seed + index), components lo + (draw mod (hi - lo + 1)) for naxes axes:
+// one 64-bit draw per 4 components (16 bits each).
+__host__ __device__ inline uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+__device__ __forceinline__ int candidate_component(uint64_t seed, long long idx, int a, int lo, int span) {
+    const uint64_t w = splitmix64(seed ^ ((uint64_t)idx * 4ull + (uint64_t)(a >> 2)) * 0xD1B54A32D192ED03ull);
+    return lo + (int)(((w >> (16 * (a & 3))) & 0xFFFFull) % (uint64_t)span);
+}
+
+__global__ void candidate_features_kernel(uint64_t seed, long long first, int n, int n_pad, int naxes, int lo,
+                                          int hi, int family, __nv_bfloat16 *X) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pad * kIn) return;
+    const int t = i / kIn, c = i % kIn;
+    float v = 0.0f;
+    if (t < n) {
+        if (c < naxes && c < 15) v = 0.25f * (float)candidate_component(seed, first + t, c, lo, hi - lo + 1);
+        else if (c >= 15 && c < 20) v = (family == c - 15) ? 1.0f : 0.0f;
+    }
+    X[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void candidate_records_kernel(uint64_t seed, const long long *idx, int n, int naxes, int lo, int hi,
+                                         const double *start, cmfw_traj_in *out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    cmfw_traj_in r;
+    for (int a = 0; a < CMFW_MAX_AXES; ++a) {
+        r.dir[a] = a < naxes ? candidate_component(seed, idx[t], a, lo, hi - lo + 1) : 0;
+        r.start[a] = a < naxes ? start[a] : 0.0;
+    }
+    out[t] = r;
+}
+
+// score[t] = H3[t] . w4 + b4, one warp per row.
+__global__ void head_forward_kernel(const __nv_bfloat16 *H, const float *w4, const float *b4, int n, float *score) {
+    const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    float s = 0.0f;
+    for (int k = lane; k < kHid; k += 32) s = fmaf(__bfloat162float(H[(size_t)row * kHid + k]), w4[k], s);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) score[row] = s + b4[0];
+}
+
+// Weighted squared error: loss = sum w (s - y)^2 / sum w, dscore = dloss/ds.
+__global__ void loss_kernel(const float *score, const float *y, const float *w, int n, float wsum, float *dscore,
+                            float *loss) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (t < n) {
+        const float r = score[t] - y[t];
+        const float wt = w ? w[t] : 1.0f;
+        dscore[t] = 2.0f * wt * r / wsum;
+        l = wt * r * r / wsum;
+    }
+    for (int o = 16; o; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l);
+}
+
+// dZ3 = (dscore w4^T) o [H3 > 0]; gw4 += dscore^T H3; gb4 += sum dscore.
+__global__ void head_backward_kernel(const __nv_bfloat16 *H, const float *w4, const float *dscore, int n,
+                                     __nv_bfloat16 *dZ, float *gw4, float *gb4) {
+    const int k = threadIdx.x;  // 256 threads: one hidden unit each
+    const int rows = (n + gridDim.x - 1) / gridDim.x;
+    const int r0 = blockIdx.x * rows, r1 = min(n, r0 + rows);
+    float acc = 0.0f, bacc = 0.0f;
+    for (int r = r0; r < r1; ++r) {
+        const float h = __bfloat162float(H[(size_t)r * kHid + k]);
+        const float d = dscore[r];
+        acc = fmaf(d, h, acc);
+        bacc += d;
+        dZ[(size_t)r * kHid + k] = __float2bfloat16_rn(h > 0.0f ? d * w4[k] : 0.0f);
+    }
+    atomicAdd(&gw4[k], acc);
+    if (k == 0) atomicAdd(gb4, bacc);
+}
+
+// Column sums of a [n x cols] bf16 matrix into g (accumulated).
+__global__ void colsum_kernel(const __nv_bfloat16 *Z, int n, int cols, float *g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    const int rows = (n + gridDim.y - 1) / gridDim.y;
+    const int r0 = blockIdx.y * rows, r1 = min(n, r0 + rows);
+    float s = 0.0f;
+    for (int r = r0; r < r1; ++r) s += __bfloat162float(Z[(size_t)r * cols + c]);
+    atomicAdd(&g[c], s);
+}
+
+// out[c][r] = in[r][c] for a rows x cols bf16 matrix (32 x 32 tiles).
+__global__ void transpose_bf16_kernel(const __nv_bfloat16 *in, int rows, int cols, __nv_bfloat16 *out) {
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = by + j, c = bx + threadIdx.x;
+        if (r < rows && c < cols) tile[j][threadIdx.x] = in[(size_t)r * cols + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int c = bx + j, r = by + threadIdx.x;
+        if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[threadIdx.x][j];
+    }
+}
+
+// Adam (beta1 0.9, beta2 0.999, eps 1e-8) on FP32 masters; refreshes the
+// BF16 copies W [rows x cols] and W^T [cols x rows] when given.
+__global__ void adam_kernel(float *p, const float *g, float *m, float *v, int n, float lr, float bc1, float bc2,
+                            int rows, int cols, __nv_bfloat16 *W, __nv_bfloat16 *WT) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = 0.9f * m[i] + 0.1f * gi;
+    const float vi = 0.999f * v[i] + 0.001f * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
+    p[i] = pi;
+    if (W) {
+        const __nv_bfloat16 b = __float2bfloat16_rn(pi);
+        W[i] = b;
+        if (WT) WT[(size_t)(i % cols) * rows + i / cols] = b;
+    }
+}
+
+__global__ void to_bf16_kernel(const float *p, int n, int rows, int cols, __nv_bfloat16 *W, __nv_bfloat16 *WT) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const __nv_bfloat16 b = __float2bfloat16_rn(p[i]);
+    W[i] = b;
+    if (WT) WT[(size_t)(i % cols) * rows + i / cols] = b;
+}
+
+// Order-preserving key of a float score (larger score -> larger key).
+__device__ __forceinline__ uint32_t score_key(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void score_hist_kernel(const float *score, long long n, uint32_t shift, uint32_t prefix,
+                                  uint32_t prefix_mask, unsigned long long *hist) {
+    __shared__ unsigned int h[2048];
+    for (int i = threadIdx.x; i < 2048; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t k = score_key(score[i]);
+        if ((k & prefix_mask) == prefix) atomicAdd(&h[(k >> shift) & 2047u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2048; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
+}
+
+__global__ void select_kernel(const float *score, long long n, uint32_t kmin, long long *out, int cap,
+                              int *count) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (score_key(score[i]) >= kmin) {
+            const int pos = atomicAdd(count, 1);
+            if (pos < cap) out[pos] = i;
+        }
+    }
+}
+
+}  // namespace cmfw
+
+using namespace cmfw;
+
+// ---- host object ------------------------------------------------------------
+
+struct cmfw_mlp {
+    int cap;  // batch capacity (multiple of 128)
+    int dev;
+    // parameters: FP32 masters, Adam state, gradients
+    float *p[8], *m[8], *v[8], *g[8];
+    int rows[8], cols[8];
+    __nv_bfloat16 *W[3], *WT[3];  // bf16 copies of W1..W3 and their transposes
+    // activations and gradients (cap x width, bf16)
+    __nv_bfloat16 *X, *H1, *H2, *H3, *dZ, *dZ2, *T1, *T2;
+    float *score, *dscore, *loss;
+    int *err;
+    long long step;
+};
+
+namespace {
+
+// parameter index: 0 W1 [256 x 64], 1 b1, 2 W2 [256 x 256], 3 b2, 4 W3, 5 b3, 6 w4 [256], 7 b4 [1]
+const int kRows[8] = {kHid, 1, kHid, 1, kHid, 1, 1, 1};
+const int kCols[8] = {kIn, kHid, kHid, kHid, kHid, kHid, kHid, 1};
+
+cmfw_status cuda_fail(cudaError_t e, const char *what) {
+    char msg[256];
+    snprintf(msg, sizeof(msg), "%s: %s", what, cudaGetErrorString(e));
+    return record_error(CMFW_ECUDA, msg);
+}
+
+size_t psize(int i) { return (size_t)kRows[i] * kCols[i]; }
+
+cudaError_t refresh_bf16(cmfw_mlp *M, cudaStream_t s) {
+    for (int l = 0; l < 3; ++l) {
+        const int n = (int)psize(2 * l);
+        to_bf16_kernel<<<(n + 255) / 256, 256, 0, s>>>(M->p[2 * l], n, kRows[2 * l], kCols[2 * l], M->W[l], M->WT[l]);
+    }
+    return cudaGetLastError();
+}
+
+GemmArgs gemm_args(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int ldb, int Mr, int N, int K, void *C,
+                   int ldc, int *err) {
+    GemmArgs g;
+    memset(&g, 0, sizeof(g));
+    g.A = A;
+    g.B = B;
+    g.M = Mr;
+    g.N = N;
+    g.K = K;
+    g.lda = lda;
+    g.ldb = ldb;
+    g.C = C;
+    g.ldc = ldc;
+    g.err = err;
+    return g;
+}
+
+// Forward pass over the first n_pad rows of M->X; H1..H3 and score filled.
+cudaError_t forward(cmfw_mlp *M, int n, int n_pad, cudaStream_t s) {
+    const __nv_bfloat16 *in = M->X;
+    __nv_bfloat16 *outs[3] = {M->H1, M->H2, M->H3};
+    int K = kIn;
+    for (int l = 0; l < 3; ++l) {
+        GemmArgs g = gemm_args(in, K, M->W[l], K, n_pad, kHid, K, outs[l], kHid, M->err);
+        g.bias = M->p[2 * l + 1];
+        cudaError_t e = gemm(g, EPI_BIAS_RELU_BF16, s);
+        if (e != cudaSuccess) return e;
+        in = outs[l];
+        K = kHid;
+    }
+    head_forward_kernel<<<(n + 7) / 8, 256, 0, s>>>(M->H3, M->p[6], M->p[7], n, M->score);
+    return cudaGetLastError();
+}
+
+cudaError_t transpose(const __nv_bfloat16 *in, int rows, int cols, __nv_bfloat16 *out, cudaStream_t s) {
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+    transpose_bf16_kernel<<<grid, block, 0, s>>>(in, rows, cols, out);
+    return cudaGetLastError();
+}
+
+// Gradients of the weighted MSE over the batch into M->g (overwritten).
+cudaError_t backward(cmfw_mlp *M, const float *y, const float *w, int n, int n_pad, float wsum, cudaStream_t s) {
+    for (int i = 0; i < 8; ++i) cudaMemsetAsync(M->g[i], 0, psize(i) * sizeof(float), s);
+    cudaMemsetAsync(M->loss, 0, sizeof(float), s);
+    cudaMemsetAsync(M->dscore, 0, sizeof(float) * n_pad, s);
+    loss_kernel<<<(n + 255) / 256, 256, 0, s>>>(M->score, y, w, n, wsum, M->dscore, M->loss);
+    cudaMemsetAsync(M->dZ, 0, (size_t)n_pad * kHid * 2, s);
+    head_backward_kernel<<<64, kHid, 0, s>>>(M->H3, M->p[6], M->dscore, n, M->dZ, M->g[6], M->g[7]);
+    // layers 3, 2, 1: dZ holds dL/dZ_l (pre-activation) of layer l
+    const __nv_bfloat16 *acts[3] = {M->X, M->H1, M->H2};  // inputs of layers 1..3
+    const __nv_bfloat16 *masks[3] = {nullptr, M->H1, M->H2};
+    __nv_bfloat16 *dz = M->dZ, *dz_next = M->dZ2;
+    for (int l = 2; l >= 0; --l) {
+        const int K_in = l == 0 ? kIn : kHid;
+        // bias gradient
+        colsum_kernel<<<dim3(1, 64), kHid, 0, s>>>(dz, n_pad, kHid, M->g[2 * l + 1]);
+        // dW_l = dZ^T [256 x n] . X^T [K_in x n]^T
+        cudaError_t e = transpose(dz, n_pad, kHid, M->T1, s);
+        if (e == cudaSuccess) e = transpose(acts[l], n_pad, K_in, M->T2, s);
+        if (e != cudaSuccess) return e;
+        GemmArgs gw = gemm_args(M->T1, n_pad, M->T2, n_pad, kHid, K_in, n_pad, M->g[2 * l], K_in, M->err);
+        e = gemm(gw, EPI_F32, s);
+        if (e != cudaSuccess) return e;
+        if (l > 0) {
+            // dZ_{l-1} = (dZ_l . W_l) o [H_{l-1} > 0]; W_l^T is [K_in x 256]
+            GemmArgs gx = gemm_args(dz, kHid, M->WT[l], kHid, n_pad, K_in, kHid, dz_next, K_in, M->err);
+            gx.mask = masks[l];
+            e = gemm(gx, EPI_MASK_BF16, s);
+            if (e != cudaSuccess) return e;
+            __nv_bfloat16 *t = dz;
+            dz = dz_next;
+            dz_next = t;
+        }
+    }
+    return cudaGetLastError();
+}
+
+cmfw_status check_batch(cmfw_mlp *M, int n) {
+    if (!M) return record_error(CMFW_EINVAL, "NULL model");
+    if (n < 0 || n > M->cap) return record_error(CMFW_EINVAL, "batch outside 0..capacity");
+    return CMFW_OK;
+}
+
+cmfw_status finish(cmfw_mlp *M, cudaError_t e, const char *what, cudaStream_t s) {
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    (void)M;
+    (void)s;
+    return CMFW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cmfw_status cmfw_mlp_create(int max_batch, uint64_t seed, cmfw_mlp **out) {
+    if (!out) return record_error(CMFW_EINVAL, "NULL output");
+    *out = nullptr;
+    if (max_batch <= 0 || max_batch > (1 << 24)) return record_error(CMFW_EINVAL, "max_batch outside 1..2^24");
+    cmfw_mlp *M = new cmfw_mlp();
+    memset(M, 0, sizeof(*M));
+    M->cap = (max_batch + 127) / 128 * 128;
+    cudaGetDevice(&M->dev);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) {
+        const size_t b = psize(i) * sizeof(float);
+        e = cudaMalloc(&M->p[i], b);
+        if (e == cudaSuccess) e = cudaMalloc(&M->m[i], b);
+        if (e == cudaSuccess) e = cudaMalloc(&M->v[i], b);
+        if (e == cudaSuccess) e = cudaMalloc(&M->g[i], b);
+        if (e == cudaSuccess) e = cudaMemset(M->m[i], 0, b);
+        if (e == cudaSuccess) e = cudaMemset(M->v[i], 0, b);
+    }
+    for (int l = 0; l < 3 && e == cudaSuccess; ++l) {
+        e = cudaMalloc(&M->W[l], psize(2 * l) * 2);
+        if (e == cudaSuccess) e = cudaMalloc(&M->WT[l], psize(2 * l) * 2);
+    }
+    const size_t act = (size_t)M->cap * kHid * 2;
+    __nv_bfloat16 **bufs[7] = {&M->H1, &M->H2, &M->H3, &M->dZ, &M->dZ2, &M->T1, &M->T2};
+    for (int i = 0; i < 7 && e == cudaSuccess; ++i) e = cudaMalloc(bufs[i], act);
+    if (e == cudaSuccess) e = cudaMalloc(&M->X, (size_t)M->cap * kIn * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&M->score, sizeof(float) * M->cap);
+    if (e == cudaSuccess) e = cudaMalloc(&M->dscore, sizeof(float) * M->cap);
+    if (e == cudaSuccess) e = cudaMalloc(&M->loss, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&M->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(M->err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        cmfw_mlp_destroy(M);
+        return record_error(CMFW_ENOMEM, "model allocation failed");
+    }
+    // He-uniform initialisation from splitmix64(seed, index); biases zero
+    std::vector<float> h;
+    for (int i = 0; i < 8; ++i) {
+        h.assign(psize(i), 0.0f);
+        const bool weight = (i % 2 == 0) || i == 6;
+        if (weight) {
+            const float fan_in = (float)kCols[i];
+            const float a = sqrtf(6.0f / fan_in);
+            for (size_t j = 0; j < h.size(); ++j) {
+                const uint64_t r = splitmix64(seed * 0x100000001B3ull + (uint64_t)i * 0x9E3779B9ull + j);
+                h[j] = a * (2.0f * (float)((r >> 11) * (1.0 / 9007199254740992.0)) - 1.0f);
+            }
+        }
+        e = cudaMemcpy(M->p[i], h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) break;
+    }
+    if (e == cudaSuccess) e = refresh_bf16(M, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cmfw_mlp_destroy(M);
+        return cuda_fail(e, "model initialisation");
+    }
+    *out = M;
+    return CMFW_OK;
+}
+
+void cmfw_mlp_destroy(cmfw_mlp *M) {
+    if (!M) return;
+    for (int i = 0; i < 8; ++i) {
+        cudaFree(M->p[i]);
+        cudaFree(M->m[i]);
+        cudaFree(M->v[i]);
+        cudaFree(M->g[i]);
+    }
+    for (int l = 0; l < 3; ++l) {
+        cudaFree(M->W[l]);
+        cudaFree(M->WT[l]);
+    }
+    __nv_bfloat16 *bufs[8] = {M->X, M->H1, M->H2, M->H3, M->dZ, M->dZ2, M->T1, M->T2};
+    for (int i = 0; i < 8; ++i) cudaFree(bufs[i]);
+    cudaFree(M->score);
+    cudaFree(M->dscore);
+    cudaFree(M->loss);
+    cudaFree(M->err);
+    delete M;
+}
+
+size_t cmfw_mlp_param_count(void) {
+    size_t n = 0;
+    for (int i = 0; i < 8; ++i) n += psize(i);
+    return n;
+}
+
+cmfw_status cmfw_mlp_get_params(cmfw_mlp *M, float *h_params) {
+    if (!M || !h_params) return record_error(CMFW_EINVAL, "NULL argument");
+    size_t off = 0;
+    for (int i = 0; i < 8; ++i) {
+        cudaError_t e = cudaMemcpy(h_params + off, M->p[i], psize(i) * sizeof(float), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(e, "parameter copy");
+        off += psize(i);
+    }
+    return CMFW_OK;
+}
+
+cmfw_status cmfw_mlp_set_params(cmfw_mlp *M, const float *h_params) {
+    if (!M || !h_params) return record_error(CMFW_EINVAL, "NULL argument");
+    size_t off = 0;
+    for (int i = 0; i < 8; ++i) {
+        cudaError_t e = cudaMemcpy(M->p[i], h_params + off, psize(i) * sizeof(float), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e, "parameter copy");
+        off += psize(i);
+    }
+    cudaError_t e = refresh_bf16(M, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? CMFW_OK : cuda_fail(e, "parameter refresh");
+}
+
+cmfw_status cmfw_mlp_forward(cmfw_mlp *M, const cmfw_traj_in *d_in, const int *d_family, int n, float *d_score,
+                             void *stream) {
+    cmfw_status st = check_batch(M, n);
+    if (st != CMFW_OK || n == 0) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n_pad = (n + 127) / 128 * 128;
+    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, n, n_pad, M->X);
+    cudaError_t e = forward(M, n, n_pad, s);
+    if (e == cudaSuccess && d_score)
+        e = cudaMemcpyAsync(d_score, M->score, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+    return finish(M, e, "mlp forward", s);
+}
+
+cmfw_status cmfw_mlp_gradients(cmfw_mlp *M, const cmfw_traj_in *d_in, const int *d_family, const float *d_target,
+                               const float *d_weight, int n, float weight_sum, float *h_grads, float *h_loss,
+                               void *stream) {
+    cmfw_status st = check_batch(M, n);
+    if (st != CMFW_OK) return st;
+    if (n == 0 || !(weight_sum > 0.0f)) return record_error(CMFW_EINVAL, "empty batch or weight sum <= 0");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n_pad = (n + 127) / 128 * 128;
+    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, n, n_pad, M->X);
+    cudaError_t e = forward(M, n, n_pad, s);
+    if (e == cudaSuccess) e = backward(M, d_target, d_weight, n, n_pad, weight_sum, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp gradients");
+    int bad = 0;
+    cudaMemcpy(&bad, M->err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (bad) return record_error(CMFW_ETIMEOUT, "a tensor-core wait gave up");
+    size_t off = 0;
+    for (int i = 0; i < 8 && h_grads; ++i) {
+        e = cudaMemcpy(h_grads + off, M->g[i], psize(i) * sizeof(float), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(e, "gradient copy");
+        off += psize(i);
+    }
+    if (h_loss) cudaMemcpy(h_loss, M->loss, sizeof(float), cudaMemcpyDeviceToHost);
+    return CMFW_OK;
+}
+
+cmfw_status cmfw_mlp_train_step(cmfw_mlp *M, const cmfw_traj_in *d_in, const int *d_family, const float *d_target,
+                                const float *d_weight, int n, float weight_sum, float lr, float *d_loss,
+                                void *stream) {
+    cmfw_status st = check_batch(M, n);
+    if (st != CMFW_OK) return st;
+    if (n == 0 || !(weight_sum > 0.0f)) return record_error(CMFW_EINVAL, "empty batch or weight sum <= 0");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n_pad = (n + 127) / 128 * 128;
+    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, n, n_pad, M->X);
+    cudaError_t e = forward(M, n, n_pad, s);
+    if (e == cudaSuccess) e = backward(M, d_target, d_weight, n, n_pad, weight_sum, s);
+    M->step += 1;
+    const float bc1 = 1.0f - powf(0.9f, (float)M->step), bc2 = 1.0f - powf(0.999f, (float)M->step);
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) {
+        const int np = (int)psize(i);
+        const bool w = (i % 2 == 0) && i < 6;
+        adam_kernel<<<(np + 255) / 256, 256, 0, s>>>(M->p[i], M->g[i], M->m[i], M->v[i], np, lr, bc1, bc2, kRows[i],
+                                                     kCols[i], w ? M->W[i / 2] : nullptr,
+                                                     w ? M->WT[i / 2] : nullptr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && d_loss) e = cudaMemcpyAsync(d_loss, M->loss, sizeof(float), cudaMemcpyDeviceToDevice, s);
+    return finish(M, e, "mlp train step", s);
+}
+
+cmfw_status cmfw_mlp_status(cmfw_mlp *M) {
+    if (!M) return record_error(CMFW_EINVAL, "NULL model");
+    int bad = 0;
+    cudaError_t e = cudaMemcpy(&bad, M->err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "status copy");
+    return bad ? record_error(CMFW_ETIMEOUT, "a tensor-core wait gave up") : CMFW_OK;
+}
+
+cmfw_status cmfw_mlp_score_candidates(cmfw_mlp *M, uint64_t seed, long long first, long long n, int naxes, int lo,
+                                      int hi, int family, float *d_scores, void *stream) {
+    if (!M || !d_scores) return record_error(CMFW_EINVAL, "NULL argument");
+    if (n < 0 || naxes < 1 || naxes > 15 || hi < lo || family < 0 || family > 4)
+        return record_error(CMFW_EINVAL, "candidate range out of bounds");
+    cudaStream_t s = (cudaStream_t)stream;
+    for (long long b = 0; b < n; b += M->cap) {
+        const int nb = (int)((n - b) < M->cap ? (n - b) : M->cap);
+        const int n_pad = (nb + 127) / 128 * 128;
+        candidate_features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(seed, first + b, nb, n_pad, naxes, lo,
+                                                                            hi, family, M->X);
+        cudaError_t e = forward(M, nb, n_pad, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_scores + b, M->score, sizeof(float) * nb, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(e, "candidate scoring");
+    }
+    return CMFW_OK;
+}
+
+cmfw_status cmfw_candidate_records(uint64_t seed, const long long *d_idx, int n, int naxes, int lo, int hi,
+                                   const double *d_start, cmfw_traj_in *d_out, void *stream) {
+    if (n < 0 || naxes < 1 || naxes > CMFW_MAX_AXES || hi < lo) return record_error(CMFW_EINVAL, "bad candidate range");
+    if (n == 0) return CMFW_OK;
+    candidate_records_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(seed, d_idx, n, naxes, lo, hi,
+                                                                                  d_start, d_out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CMFW_OK : cuda_fail(e, "candidate records");
+}
+
+cmfw_status cmfw_select_top(const float *d_scores, long long n, long long k, long long *d_idx, int cap, int *h_count,
+                            void *stream) {
+    if (!d_scores || !d_idx || !h_count || k < 1 || cap < 1) return record_error(CMFW_EINVAL, "bad selection arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long *d_hist = nullptr;
+    int *d_count = nullptr;
+    cudaError_t e = cudaMalloc(&d_hist, 2048 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&d_count, sizeof(int));
+    // radix select of the k-th largest key: 11 + 11 + 10 bits
+    uint32_t prefix = 0, mask = 0;
+    long long need = k;
+    const uint32_t shifts[3] = {21, 10, 0};
+    const uint32_t widths[3] = {11, 11, 10};
+    std::vector<unsigned long long> h(2048);
+    for (int pass = 0; pass < 3 && e == cudaSuccess; ++pass) {
+        e = cudaMemsetAsync(d_hist, 0, 2048 * sizeof(unsigned long long), s);
+        if (e != cudaSuccess) break;
+        score_hist_kernel<<<592, 256, 0, s>>>(d_scores, n, shifts[pass], prefix, mask, d_hist);
+        e = cudaMemcpyAsync(h.data(), d_hist, 2048 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) break;
+        const int nb = 1 << widths[pass];
+        int b = nb - 1;
+        for (; b > 0; --b) {
+            if ((long long)h[b] >= need) break;
+            need -= (long long)h[b];
+        }
+        prefix |= (uint32_t)b << shifts[pass];
+        mask |= (uint32_t)(nb - 1) << shifts[pass];
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, sizeof(int), s);
+    if (e == cudaSuccess) {
+        select_kernel<<<592, 256, 0, s>>>(d_scores, n, prefix, d_idx, cap, d_count);
+        e = cudaMemcpyAsync(h_count, d_count, sizeof(int), cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_hist);
+    cudaFree(d_count);
+    return e == cudaSuccess ? CMFW_OK : cuda_fail(e, "top-k selection");
+}
+
+}  // extern "C"

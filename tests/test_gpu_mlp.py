@@ -1,0 +1,99 @@
+"""Learned proposal network on the tensor cores (marked gpu): forward pass
+and gradients of the library's tcgen05 kernels against the CPU reference
+(oracle/mlp_ref.py, same BF16 roundings), training progress, the seeded
+candidate generator and the top-k selection."""
+import numpy as np
+import pytest
+
+import cmfw
+from cmfw import mlp as cm
+from oracle import mlp_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(n, seed):
+    rng = np.random.default_rng(seed)
+    recs = np.zeros(n, dtype=cmfw.IN_DTYPE)
+    recs["dir"][:, :15] = rng.integers(0, 5, (n, 15))
+    fam = rng.integers(0, 5, n).astype(np.int32)
+    return recs, fam
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def test_forward_and_gradients_match_reference(cuda):
+    torch = cuda
+    m = cm.Mlp(512, seed=3)
+    params = mlp_ref.unflatten(m.get_params())
+    n = 300  # not a multiple of 128: padded rows must not leak into results
+    recs, fam = _batch(n, 1)
+    d_in, d_fam = cmfw.to_device(recs), torch.from_numpy(fam).cuda()
+    X = mlp_ref.features(recs["dir"], fam)
+    s_ref, _ = mlp_ref.forward(params, X)
+    s = m.forward(d_in, d_fam, n).cpu().numpy()
+    assert _rel(s, s_ref) < 1e-2, _rel(s, s_ref)
+    rng = np.random.default_rng(2)
+    y = rng.normal(0, 1, n).astype(np.float32)
+    w = rng.uniform(0.5, 2.0, n).astype(np.float32)
+    g, loss = m.gradients(d_in, d_fam, torch.from_numpy(y).cuda(), torch.from_numpy(w).cuda(), n, float(w.sum()))
+    loss_ref, g_ref = mlp_ref.gradients(params, X, y, w, float(w.sum()))
+    assert abs(loss - loss_ref) <= 1e-2 * abs(loss_ref)
+    for name, a, b in zip(["W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4"], mlp_ref.unflatten(g),
+                          mlp_ref.unflatten(g_ref)):
+        assert _rel(a, b) < 3e-2, (name, _rel(a, b))
+    m.status()
+
+
+def test_training_reduces_loss(cuda):
+    torch = cuda
+    m = cm.Mlp(1024, seed=5)
+    n = 1024
+    recs, fam = _batch(8 * n, 7)
+    d = recs["dir"][:, :15].astype(np.float32)
+    y = (0.3 * (d[:, 0] - d[:, 3]) + 0.2 * np.maximum(d[:, 5] - 2, 0) + 0.1 * fam).astype(np.float32)
+    d_in, d_fam, d_y = cmfw.to_device(recs), torch.from_numpy(fam).cuda(), torch.from_numpy(y).cuda()
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    first = None
+    for it in range(400):
+        lo = (it % 8) * n
+        m.train_step(d_in[lo:lo + n], d_fam[lo:lo + n], d_y[lo:lo + n], None, n, float(n), 2e-3, loss)
+        if it == 0:
+            first = float(loss.item())
+    _, last = m.gradients(d_in[:n], d_fam[:n], d_y[:n], None, n, float(n))
+    assert last < 0.05 * first, (first, last)
+    m.status()
+
+
+def _splitmix64(x):
+    x = (x + np.uint64(0x9E3779B97F4A7C15)) & np.uint64(0xFFFFFFFFFFFFFFFF)
+    x = ((x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & np.uint64(0xFFFFFFFFFFFFFFFF)
+    x = ((x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & np.uint64(0xFFFFFFFFFFFFFFFF)
+    return x ^ (x >> np.uint64(31))
+
+
+def test_candidates_and_selection(cuda):
+    torch = cuda
+    seed, naxes, lo, hi = 12345, 15, 0, 4
+    m = cm.Mlp(4096, seed=9)
+    idx = torch.arange(0, 3000, dtype=torch.int64, device="cuda")
+    recs = cm.candidate_records(seed, idx, naxes, lo, hi, [1.0] * 8 + [2.0] * 7)
+    host = recs.cpu().numpy().reshape(-1).view(cmfw.IN_DTYPE)
+    with np.errstate(over="ignore"):
+        i = np.arange(3000, dtype=np.uint64)[:, None]
+        a = np.arange(naxes, dtype=np.uint64)[None, :]
+        draw = _splitmix64(np.uint64(seed) ^ ((i * np.uint64(4) + (a >> np.uint64(2))) * np.uint64(0xD1B54A32D192ED03)))
+        comp = lo + ((draw >> (np.uint64(16) * (a & np.uint64(3)))) & np.uint64(0xFFFF)) % np.uint64(hi - lo + 1)
+    assert (host["dir"][:, :naxes] == comp.astype(np.int32)).all()
+    assert (host["start"][:, :15] == [1.0] * 8 + [2.0] * 7).all()
+    fam = torch.full((3000,), 4, dtype=torch.int32, device="cuda")
+    a = m.forward(recs, fam, 3000)
+    b = m.score_candidates(seed, 0, 3000, naxes, lo, hi, 4)
+    assert torch.equal(a, b)
+    # top-k over a million scores against a full sort
+    rng = np.random.default_rng(4)
+    sc = rng.normal(0, 1, 1_000_003).astype(np.float32)
+    top = cm.select_top(torch.from_numpy(sc).cuda(), 1000).cpu().numpy()
+    assert sorted(top.tolist()) == sorted(np.argsort(-sc)[:1000].tolist())
