@@ -10,9 +10,11 @@
 //     here (zeta starts hit a singular lead coefficient on their first y+
 //     step), and leave after a handful of steps. Survivors store their
 //     prefix product and append their index to a list.
-//  2. chunk: one CTA of NT threads (256 up to rank 6, else 128) per
-//     survivor, on a persistent grid (SMs x resident CTAs) that strides
-//     over the survivor list. The remaining steps form three segments [S+1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the snapshot
+//  2. chunk: clusters of 2 CTAs of NT threads (256 up to rank 6, else 128)
+//     on a persistent grid that strides over the survivor list; each
+//     survivor is walked by one CTA, or by both CTAs of a cluster when there
+//     are fewer survivors than half the CTAs (the parts are multiplied in
+//     order through distributed shared memory). The remaining steps form three segments [S+1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the snapshot
 //     depths are segment ends); each thread walks a contiguous run of lattice
 //     steps of one segment with the same registers-only step as the
 //     sequential kernel, the runs of a segment are multiplied in order by a
@@ -36,7 +38,11 @@
 // in the sequential walk. CMFW_F_PLAIN_RUNS selects plain-FP64 runs (fewer
 // instructions, no such guarantee); df64 runs in float-float with FP64
 // products (ArithFF).
+#include <cooperative_groups.h>
+
 #include "walk_arith.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace cmfw {
 
@@ -95,9 +101,15 @@ __global__ void __launch_bounds__(128) walk_prefix_kernel(ChunkArgs C) {
 // 6), 128 above.
 __host__ __device__ constexpr int chunk_threads(int dim) { return dim <= 6 ? 256 : 128; }
 
+// CTAs per cluster of the chunk kernel: a trajectory is walked by one CTA,
+// or by both CTAs of a cluster when the survivors leave enough SMs (chosen
+// on the device from the number of survivors).
+constexpr int kChunkCluster = 2;
+
 template <int P_, int Q_, int DIM, class A>
 __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArgs C) {
     constexpr int NT = chunk_threads(DIM);
+    constexpr int CL = kChunkCluster;
     typedef typename A::T T;
     typedef typename A::Combine CA;
     typedef typename CA::T CT;
@@ -107,52 +119,61 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
     constexpr int QM = (P_ > 0) ? Q_ : 7;
     constexpr int DD = DIM * DIM;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    CT *smem = (CT *)smem_raw;                  // NT partial products + 3 snapshots
-    int *sexp = (int *)(smem + (NT + 3) * DD);  // NT exponents
-    // earliest failing lattice step of the trajectory, as step * 16 + status
+    CT *smem = (CT *)smem_raw;                  // NT run products + 6 work matrices
+    int *sexp = (int *)(smem + (NT + 6) * DD);  // NT exponents
+    // earliest failing lattice step of this CTA's runs, as step * 16 + status
     __shared__ int s_fail;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
     const int tid = threadIdx.x;
     const int P = (P_ > 0) ? P_ : W.p;
     const int Q = (P_ > 0) ? Q_ : W.q;
     const int naxes = P + Q;
     const StepConst K = make_step_const(P, Q, DIM, W.z);
 
-    // segments of lattice steps and the threads that walk them (the same
-    // for every trajectory of the launch)
+    // parts per trajectory: as many CTAs as the survivors leave room for
+    const int count = *C.count;
+    const int nclusters = gridDim.x / CL;
+    const int NP = (count * CL <= (int)gridDim.x) ? CL : 1;
+    const int per_cluster = CL / NP;
+    const int part = crank % NP, sub = crank / NP;
+    const int NTOT = NT * NP;
+
+    // segments of lattice steps and the runs (global index g over the NP
+    // CTAs) that cover them; the same for every trajectory of the launch
     const int S = min(C.prefix_steps, W.N - 2 * W.h - 1);
     const int cp1 = W.N - 2 * W.h, cp2 = W.N - W.h;
     const int L0 = cp1 - S, L1 = W.h, L2 = W.h;
     const int rest = W.N - S;
-    int T1 = (NT * L1 + rest / 2) / rest;
+    int T1 = (NTOT * L1 + rest / 2) / rest;
     T1 = max(1, min(T1, L1));
     int T2 = max(1, min(T1, L2));
-    const int T0 = NT - T1 - T2;
-    const int seg = tid < T0 ? 0 : (tid < T0 + T1 ? 1 : 2);
-    const int base = seg == 0 ? 0 : (seg == 1 ? T0 : T0 + T1);
-    const int Tseg = seg == 0 ? T0 : (seg == 1 ? T1 : T2);
+    const int T0 = NTOT - T1 - T2;
+    const int segbase[3] = {0, T0, T0 + T1}, segT[3] = {T0, T1, T2};
+    const int g = part * NT + tid;
+    const int seg = g < T0 ? 0 : (g < T0 + T1 ? 1 : 2);
     const int Lseg = seg == 0 ? L0 : (seg == 1 ? L1 : L2);
     const int first = seg == 0 ? S + 1 : (seg == 1 ? cp1 + 1 : cp2 + 1);
-    const int local = tid - base;
-    const int lo = first + (int)(((long long)local * Lseg) / Tseg);
-    const int hi = first + (int)(((long long)(local + 1) * Lseg) / Tseg);
-    const int Tmax = max(T0, max(T1, T2));
-    const int count = *C.count;
-
-    // persistent: CTAs stride over the survivors
-    for (int b = blockIdx.x; b < count; b += gridDim.x) {
-        const int t = C.list[b];
-        const cmfw_traj_in &in = W.in[t];
-        int absd[NAX];
-        uint32_t neg;
-        const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
-        if (tid == 0) s_fail = 0x7fffffff;
-
-        double pos[NAX];
+    const int local = g - segbase[seg];
+    const int lo = first + (int)(((long long)local * Lseg) / segT[seg]);
+    const int hi = first + (int)(((long long)(local + 1) * Lseg) / segT[seg]);
+    // this CTA's share [cbeg, cend) of each segment's runs, in CTA thread ids
+    int cbeg[3], ccnt[3];
 #pragma unroll
-        for (int a = 0; a < NAX; ++a) {
-            const double d = (a < naxes) ? (double)in.dir[a] : 0.0;
-            pos[a] = (a < naxes) ? in.start[a] + (double)(lo - 1) * d : 0.0;
-        }
+    for (int k = 0; k < 3; ++k) {
+        const int b0 = max(segbase[k], part * NT), b1 = min(segbase[k] + segT[k], (part + 1) * NT);
+        cbeg[k] = b0 - part * NT;
+        ccnt[k] = max(0, b1 - b0);
+    }
+    const int lrel = tid - cbeg[seg];  // index among this CTA's runs of the segment
+
+    for (int round = 0;; ++round) {
+        const int b0 = (round * nclusters + (int)(blockIdx.x / CL)) * per_cluster;
+        if (b0 >= count) break;  // uniform over the cluster
+        const int b = b0 + sub;
+        const bool active = b < count;
+        const int t = active ? C.list[b] : 0;
+        if (tid == 0) s_fail = 0x7fffffff;
         T m[DIM][DIM];
         int ex[DIM];
 #pragma unroll
@@ -162,61 +183,97 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
             for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r == j) ? 1.0 : 0.0);
         }
         __syncthreads();
-        volatile int *fail = &s_fail;
-        for (int step = lo; step < hi; ++step) {
-            if (*fail < step * 16) break;  // an earlier step failed: this run is moot
-            int st = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
-            if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
-            if (st != CMFW_TRAJ_OK) {
-                atomicMin(&s_fail, step * 16 + st);
-                break;
+        if (active) {
+            const cmfw_traj_in &in = W.in[t];
+            int absd[NAX];
+            uint32_t neg;
+            const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
+            double pos[NAX];
+#pragma unroll
+            for (int a = 0; a < NAX; ++a) {
+                const double d = (a < naxes) ? (double)in.dir[a] : 0.0;
+                pos[a] = (a < naxes) ? in.start[a] + (double)(lo - 1) * d : 0.0;
+            }
+            volatile int *fail = &s_fail;
+            for (int step = lo; step < hi; ++step) {
+                if (*fail < step * 16) break;  // an earlier step failed: this run is moot
+                int st = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
+                if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
+                if (st != CMFW_TRAJ_OK) {
+                    atomicMin(&s_fail, step * 16 + st);
+                    break;
+                }
             }
         }
         sexp[tid] = to_matrix_exponent<DIM, A>(m, ex, smem + tid * DD);
         __syncthreads();
-        const int fkey = s_fail;
-        if (fkey != 0x7fffffff) {
-            if (tid == 0) write_invalid(W, t, fkey & 15);
-            __syncthreads();  // s_fail and the products are reused
-            continue;
-        }
-        // in-order tree product of each segment's runs
-        for (int stride = 1; stride < Tmax; stride <<= 1) {
-            if ((local % (2 * stride)) == 0 && local + stride < Tseg)
+        // in-order tree product of this CTA's runs of each segment
+        for (int stride = 1; stride < NT; stride <<= 1) {
+            if (active && (lrel % (2 * stride)) == 0 && lrel + stride < ccnt[seg])
                 sexp[tid] = mat_mul_exp<DIM, CA>(smem + tid * DD, sexp[tid], smem + (tid + stride) * DD,
                                                  sexp[tid + stride], smem + tid * DD);
             __syncthreads();
         }
-        if (tid == 0) {
-            // snapshots: prefix * seg0, then * seg1, then * seg2
-            CT *x = smem + NT * DD;
-            const int e = mat_mul_exp<DIM, CA>((const CT *)C.pre + (size_t)t * DD, C.pre_e[t], smem, sexp[0], x);
-            const int e1 = mat_mul_exp<DIM, CA>(x, e, smem + T0 * DD, sexp[T0], x + DD);
-            const int e2 = mat_mul_exp<DIM, CA>(x + DD, e1, smem + (T0 + T1) * DD, sexp[T0 + T1], x + 2 * DD);
-            double *snap = W.snap + (size_t)t * 3 * DD;
-            int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
-            const int es[3] = {e, e1, e2};
-            bool ok = true;
-            for (int k = 0; k < 3; ++k) {
-                bool nz = false;
-                for (int i = 0; i < DD; ++i) {
-                    const double v = CA::to(x[k * DD + i]);
-                    snap[k * DD + i] = v;
-                    ok &= isfinite(v);
-                    nz |= v != 0.0;
-                }
-                ok &= nz;
-                for (int r = 0; r < DIM; ++r) snap_e[k * DIM + r] = es[k];
-            }
-            if (!ok) {
-                write_invalid(W, t, CMFW_TRAJ_NONFINITE);
+        // every part's products and failure key are final (CTAs that walk
+        // alone need no cluster barrier)
+        if (NP > 1) cluster.sync();
+        if (active && part == 0 && tid == 0) {
+            // the leader combines the parts in order, then the snapshots
+            int fkey = 0x7fffffff;
+            for (int q = 0; q < NP; ++q) fkey = min(fkey, *cluster.map_shared_rank(&s_fail, crank + q));
+            if (fkey != 0x7fffffff) {
+                write_invalid(W, t, fkey & 15);
             } else {
-                double ls[3];
-                for (int k = 0; k < 3; ++k) ls[k] = normalise_rows(snap + k * DD, snap_e + k * DIM, DIM, 0.0);
-                finish_valid(W, t, snap, DIM, ls);
+                CT *y = smem + NT * DD, *x = y + 3 * DD;
+                int ye[3];
+                for (int k = 0; k < 3; ++k) {
+                    bool have = false;
+                    for (int q = 0; q < NP; ++q) {
+                        const int b0q = max(segbase[k], q * NT), b1q = min(segbase[k] + segT[k], (q + 1) * NT);
+                        if (b1q <= b0q) continue;
+                        const int slot = b0q - q * NT;
+                        CT *pm = cluster.map_shared_rank(smem, crank + q) + slot * DD;
+                        const int pe = *cluster.map_shared_rank(sexp + slot, crank + q);
+                        if (!have) {
+                            for (int i = 0; i < DD; ++i) y[k * DD + i] = pm[i];
+                            ye[k] = pe;
+                            have = true;
+                        } else {
+                            ye[k] = mat_mul_exp<DIM, CA>(y + k * DD, ye[k], pm, pe, y + k * DD);
+                        }
+                    }
+                }
+                const int e = mat_mul_exp<DIM, CA>((const CT *)C.pre + (size_t)t * DD, C.pre_e[t], y, ye[0], x);
+                const int e1 = mat_mul_exp<DIM, CA>(x, e, y + DD, ye[1], x + DD);
+                const int e2 = mat_mul_exp<DIM, CA>(x + DD, e1, y + 2 * DD, ye[2], x + 2 * DD);
+                double *snap = W.snap + (size_t)t * 3 * DD;
+                int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
+                const int es[3] = {e, e1, e2};
+                bool ok = true;
+                for (int k = 0; k < 3; ++k) {
+                    bool nz = false;
+                    for (int i = 0; i < DD; ++i) {
+                        const double v = CA::to(x[k * DD + i]);
+                        snap[k * DD + i] = v;
+                        ok &= isfinite(v);
+                        nz |= v != 0.0;
+                    }
+                    ok &= nz;
+                    for (int r = 0; r < DIM; ++r) snap_e[k * DIM + r] = es[k];
+                }
+                if (!ok) {
+                    write_invalid(W, t, CMFW_TRAJ_NONFINITE);
+                } else {
+                    double ls[3];
+                    for (int k = 0; k < 3; ++k) ls[k] = normalise_rows(snap + k * DD, snap_e + k * DIM, DIM, 0.0);
+                    finish_valid(W, t, snap, DIM, ls);
+                }
             }
         }
-        __syncthreads();  // shared products are reused by the next trajectory
+        if (NP > 1)
+            cluster.sync();  // the leader has read every part's shared memory
+        else
+            __syncthreads();  // shared products are reused by the next trajectory
     }
 }
 
@@ -269,21 +326,40 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     C.count = (int *)p;
     C.prefix_steps = prefix_steps;
     const int NT = chunk_threads(dim);
-    const size_t shmem = (size_t)(NT + 3) * dim * dim * sizeof(typename A::Combine::T) + NT * sizeof(int);
+    const size_t shmem = (size_t)(NT + 6) * dim * dim * sizeof(typename A::Combine::T) + NT * sizeof(int);
     cudaError_t e = cudaFuncSetAttribute((const void *)k.chunk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shmem);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(C.count, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 148, per_sm = 1;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k.chunk, NT, shmem) != cudaSuccess ||
-        per_sm < 1)
-        per_sm = 1;
-    const int grid = max(1, min(n, sms * per_sm));
     k.prefix<<<(n + 127) / 128, 128, 0, s>>>(C);
-    k.chunk<<<grid, NT, shmem, s>>>(C);
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // persistent grid of 2-CTA clusters: as many as can be resident at once
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kChunkCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = shmem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cfg.gridDim = dim3((unsigned)(sms / kChunkCluster * kChunkCluster), 1, 1);
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, (const void *)k.chunk, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        clusters = sms / kChunkCluster;
+    }
+    const int need = (n + kChunkCluster - 1) / kChunkCluster;  // one trajectory per CTA at most
+    clusters = max(1, min(clusters, need));
+    cfg.gridDim = dim3((unsigned)(clusters * kChunkCluster), 1, 1);
+    e = cudaLaunchKernelEx(&cfg, k.chunk, C);
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 // ff selects the df64 walk (float-float runs); otherwise the f64 walk with
