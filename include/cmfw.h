@@ -301,6 +301,13 @@ cmfw_status cmfw_mlp_status(cmfw_mlp *mlp);
  * with the network (family one-hot `family`) into d_scores[0..n). */
 cmfw_status cmfw_mlp_score_candidates(cmfw_mlp *mlp, uint64_t seed, long long first, long long n, int naxes,
                                       int lo, int hi, int family, float *d_scores, void *stream);
+/* The same scores in one launch: clusters of two CTAs keep the three
+ * hidden layers' weights resident in shared memory (each CTA half of every
+ * layer), generate the candidates' features in place and exchange the
+ * activation halves through distributed shared memory. */
+cmfw_status cmfw_mlp_score_candidates_fused(cmfw_mlp *mlp, uint64_t seed, long long first, long long n,
+                                            int naxes, int lo, int hi, int family, float *d_scores,
+                                            void *stream);
 /* Records of the candidates d_idx[0..n) of the same generator, start d_start. */
 cmfw_status cmfw_candidate_records(uint64_t seed, const long long *d_idx, int n, int naxes, int lo, int hi,
                                    const double *d_start, cmfw_traj_in *d_out, void *stream);

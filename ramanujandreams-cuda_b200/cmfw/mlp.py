@@ -82,12 +82,15 @@ class Mlp:
     def status(self):
         check(lib().cmfw_mlp_status(self.h))
 
-    def score_candidates(self, seed, first, n, naxes, lo, hi, family, d_scores=None, stream=None):
+    def score_candidates(self, seed, first, n, naxes, lo, hi, family, d_scores=None, stream=None, fused=True):
+        """Scores of candidates first .. first+n-1: one fused launch (default)
+        or per-layer tensor-core GEMMs through the activation buffers."""
         torch = api._torch()
         if d_scores is None:
             d_scores = torch.empty(max(n, 1), dtype=torch.float32, device="cuda")
-        check(lib().cmfw_mlp_score_candidates(self.h, ctypes.c_uint64(seed), int(first), int(n), int(naxes), int(lo),
-                                              int(hi), int(family), _ptr(d_scores), api._stream_handle(stream)))
+        fn = lib().cmfw_mlp_score_candidates_fused if fused else lib().cmfw_mlp_score_candidates
+        check(fn(self.h, ctypes.c_uint64(seed), int(first), int(n), int(naxes), int(lo), int(hi), int(family),
+                 _ptr(d_scores), api._stream_handle(stream)))
         return d_scores[:n]
 
 

@@ -26,6 +26,9 @@
 #include "cmfw_internal.cuh"
 #include "tc_sm100.cuh"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 namespace cmfw {
 cmfw_status record_error(cmfw_status s, const char *msg);
 
@@ -371,6 +374,188 @@ __global__ void select_kernel(const float *score, long long n, uint32_t kmin, lo
     }
 }
 
+// ---- fused scoring ----------------------------------------------------------
+//
+// Scoring a large candidate set in one launch: clusters of two CTAs stride
+// over 128-candidate tiles. CTA r of a cluster owns hidden features
+// [128 r, 128 r + 128) of every layer and keeps its halves of W1, W2, W3
+// (16 + 64 + 64 KB, interleaved K-major) in shared memory for the whole
+// launch, so weights are read from HBM once per CTA. Per tile: the
+// candidates' features are generated in place (no records), then per layer
+// one thread issues the M = 128, N = 128 tcgen05 MMAs into a 128-column TMEM
+// accumulator; after the cluster barrier that ends both CTAs' MMAs, 256
+// threads load the accumulator, add the bias, apply ReLU, round to BF16 and
+// write their half of the activations into both CTAs' activation tiles
+// (the peer's through distributed shared memory); a second barrier makes the
+// tile complete on both sides. The head's 256-term dot product is split the
+// same way and summed in CTA 0.
+
+struct FusedArgs {
+    const __nv_bfloat16 *W[3];  // [256 x 64], [256 x 256], [256 x 256] row-major
+    const float *bias[3];       // 256 each
+    const float *w4, *b4;
+    uint64_t seed;
+    long long first, n;
+    int naxes, lo, hi, family;
+    float *score;
+    int *err;
+};
+
+constexpr int kFusedSmem = 16384 + 65536 + 65536 + 65536 + 4 * 128 * 4 + 4 * 128 * 4;
+
+__device__ __forceinline__ void fence_async_cluster() {
+    asm volatile("fence.proxy.async.shared::cluster;" ::: "memory");
+}
+
+// Rows [row0, row0 + rows) of a row-major [* x K] bf16 matrix into an
+// interleaved K-major tile.
+__device__ __forceinline__ void load_tile(unsigned char *dst, const __nv_bfloat16 *src, int row0, int rows, int K) {
+    const int chunks = rows * (K / 8);
+    for (int i = threadIdx.x; i < chunks; i += blockDim.x) {
+        const int r = i / (K / 8), c = i % (K / 8);
+        *(uint4 *)(dst + tc::tile_offset(r, c * 8, K)) = *(const uint4 *)(src + (size_t)(row0 + r) * K + c * 8);
+    }
+}
+
+// Eight consecutive activations (columns k .. k+7 of one row) as a 16-byte chunk.
+__device__ __forceinline__ uint4 pack8(const float *v) {
+    __nv_bfloat162 h[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+    return *(uint4 *)h;
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256) mlp_score_fused_kernel(FusedArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *w1 = smem;                 // 128 x 64
+    unsigned char *w2 = w1 + 16384;           // 128 x 256
+    unsigned char *w3 = w2 + 65536;           // 128 x 256
+    unsigned char *act = w3 + 65536;          // 128 x 256 (128 x 64 for the features)
+    float *sbias = (float *)(act + 65536);    // 3 x 128 biases, then 128 of w4
+    // head partial sums: [0, 256) per column half, [256, 384) this CTA's
+    // half (CTA 0), [384, 512) CTA 1's half (written by CTA 1)
+    float *spart = sbias + 4 * 128;
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_bad;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int r = (int)cluster.block_rank();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char *peer_act = cluster.map_shared_rank(act, r ^ 1);
+    float *peer_part0 = cluster.map_shared_rank(spart, 0);
+
+    // resident weights and biases of this CTA's half
+    load_tile(w1, a.W[0], 128 * r, 128, kIn);
+    load_tile(w2, a.W[1], 128 * r, 128, kHid);
+    load_tile(w3, a.W[2], 128 * r, 128, kHid);
+    for (int i = threadIdx.x; i < 128; i += blockDim.x) {
+        for (int l = 0; l < 3; ++l) sbias[l * 128 + i] = a.bias[l][128 * r + i];
+        sbias[3 * 128 + i] = a.w4[128 * r + i];
+    }
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        s_bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_base, 128);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_base;
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 128);
+    const uint32_t s_act = tc::smem_u32(act), s_w[3] = {tc::smem_u32(w1), tc::smem_u32(w2), tc::smem_u32(w3)};
+    uint32_t uses = 0;
+    bool ok = true;
+    const long long ntiles = (a.n + 127) / 128;
+    const int nclusters = gridDim.x / 2;
+    const int span = a.hi - a.lo + 1;
+    const int trow = (warp & 3) * 32 + lane;  // accumulator lane = tile row
+    const int tcol = (warp >> 2) * 64;        // this thread's 64 accumulator columns
+
+    for (long long tile = blockIdx.x / 2; tile < ntiles; tile += nclusters) {
+        // features of the tile's candidates (K = 64 layout)
+        for (int i = threadIdx.x; i < 128 * 8; i += blockDim.x) {
+            const int row = i >> 3, c = i & 7;
+            const long long cand = tile * 128 + row;
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int f = 8 * c + j;
+                float x = 0.0f;
+                if (cand < a.n) {
+                    if (f < a.naxes && f < 15) x = 0.25f * (float)candidate_component(a.seed, a.first + cand, f, a.lo, span);
+                    else if (f >= 15 && f < 20) x = (a.family == f - 15) ? 1.0f : 0.0f;
+                }
+                v[j] = x;
+            }
+            *(uint4 *)(act + tc::tile_offset(row, 8 * c, kIn)) = pack8(v);
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        for (int l = 0; l < 3; ++l) {
+            const int K = l == 0 ? kIn : kHid;
+            if (threadIdx.x == 0) {
+                tc::fence_after_sync();
+                for (int j = 0; j < K / 16; ++j)
+                    tc::mma_bf16(tmem, tc::smem_desc(s_act + j * 256, 128, K * 16),
+                                 tc::smem_desc(s_w[l] + j * 256, 128, K * 16), idesc, j > 0);
+                tc::commit(&bar);
+            }
+            if (!tc::mbar_wait(&bar, uses & 1)) ok = false;
+            ++uses;
+            tc::fence_after_sync();
+            // both CTAs' MMAs have read their activation tiles
+            tc::fence_before_sync();
+            cluster.sync();
+            tc::fence_after_sync();
+            float v[64];
+            tc::tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)tcol, *(float(*)[32])v);
+            tc::tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(tcol + 32), *(float(*)[32])(v + 32));
+            const float *b = sbias + l * 128 + tcol;
+#pragma unroll
+            for (int i = 0; i < 64; ++i) v[i] = fmaxf(v[i] + b[i], 0.0f);
+            if (l < 2) {
+                // this half of the next layer's input, into both CTAs
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const uint4 q = pack8(v + 8 * c);
+                    const uint32_t off = tc::tile_offset(trow, 128 * r + tcol + 8 * c, kHid);
+                    *(uint4 *)(act + off) = q;
+                    *(uint4 *)(peer_act + off) = q;
+                }
+                fence_async_cluster();
+                tc::fence_before_sync();
+                cluster.sync();
+            } else {
+                // head: this CTA's 128 of the 256 terms, on the BF16-rounded activations
+                float sum = 0.0f;
+#pragma unroll
+                for (int i = 0; i < 64; ++i) sum = fmaf(__bfloat162float(__float2bfloat16_rn(v[i])), sbias[384 + tcol + i], sum);
+                spart[(warp >> 2) * 128 + trow] = sum;
+                __syncthreads();
+                if (threadIdx.x < 128) {
+                    const float half = spart[threadIdx.x] + spart[128 + threadIdx.x];
+                    if (r == 1) peer_part0[384 + threadIdx.x] = half;
+                    else spart[256 + threadIdx.x] = half;
+                }
+                tc::fence_before_sync();
+                cluster.sync();
+                if (r == 0 && threadIdx.x < 128) {
+                    const long long cand = tile * 128 + threadIdx.x;
+                    if (cand < a.n) a.score[cand] = spart[256 + threadIdx.x] + spart[384 + threadIdx.x] + a.b4[0];
+                }
+            }
+        }
+    }
+    if (!ok) s_bad = 1;
+    __syncthreads();
+    if (s_bad && threadIdx.x == 0) atomicExch(a.err, 1);
+    tc::fence_before_sync();
+    cluster.sync();  // no peer writes into this CTA's shared memory after here
+    if (warp == 0) tc::tmem_dealloc(tmem, 128);
+}
+
 }  // namespace cmfw
 
 using namespace cmfw;
@@ -708,6 +893,54 @@ cmfw_status cmfw_mlp_score_candidates(cmfw_mlp *M, uint64_t seed, long long firs
         if (e != cudaSuccess) return cuda_fail(e, "candidate scoring");
     }
     return CMFW_OK;
+}
+
+cmfw_status cmfw_mlp_score_candidates_fused(cmfw_mlp *M, uint64_t seed, long long first, long long n, int naxes,
+                                            int lo, int hi, int family, float *d_scores, void *stream) {
+    if (!M || !d_scores) return record_error(CMFW_EINVAL, "NULL argument");
+    if (n < 0 || naxes < 1 || naxes > 15 || hi < lo || family < 0 || family > 4)
+        return record_error(CMFW_EINVAL, "candidate range out of bounds");
+    if (n == 0) return CMFW_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaFuncSetAttribute((const void *)mlp_score_fused_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem);
+    if (e != cudaSuccess) return cuda_fail(e, "fused scoring attributes");
+    FusedArgs a;
+    for (int l = 0; l < 3; ++l) {
+        a.W[l] = M->W[l];
+        a.bias[l] = M->p[2 * l + 1];
+    }
+    a.w4 = M->p[6];
+    a.b4 = M->p[7];
+    a.seed = seed;
+    a.first = first;
+    a.n = n;
+    a.naxes = naxes;
+    a.lo = lo;
+    a.hi = hi;
+    a.family = family;
+    a.score = d_scores;
+    a.err = M->err;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(sms / 2 * 2), 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = kFusedSmem;
+    cfg.stream = s;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, (const void *)mlp_score_fused_kernel, &cfg) != cudaSuccess ||
+        clusters < 1) {
+        cudaGetLastError();
+        clusters = sms / 2;
+    }
+    const long long tiles = (n + 127) / 128;
+    if ((long long)clusters > tiles) clusters = (int)tiles;
+    cfg.gridDim = dim3((unsigned)(2 * clusters), 1, 1);
+    e = cudaLaunchKernelEx(&cfg, mlp_score_fused_kernel, a);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e == cudaSuccess ? CMFW_OK : cuda_fail(e, "fused scoring launch");
 }
 
 cmfw_status cmfw_candidate_records(uint64_t seed, const long long *d_idx, int n, int naxes, int lo, int hi,

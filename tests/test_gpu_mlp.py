@@ -90,10 +90,24 @@ def test_candidates_and_selection(cuda):
     assert (host["start"][:, :15] == [1.0] * 8 + [2.0] * 7).all()
     fam = torch.full((3000,), 4, dtype=torch.int32, device="cuda")
     a = m.forward(recs, fam, 3000)
-    b = m.score_candidates(seed, 0, 3000, naxes, lo, hi, 4)
-    assert torch.equal(a, b)
+    b = m.score_candidates(seed, 0, 3000, naxes, lo, hi, 4, fused=False)
+    assert torch.equal(a, b)  # same features, same kernels
     # top-k over a million scores against a full sort
     rng = np.random.default_rng(4)
     sc = rng.normal(0, 1, 1_000_003).astype(np.float32)
     top = cm.select_top(torch.from_numpy(sc).cuda(), 1000).cpu().numpy()
     assert sorted(top.tolist()) == sorted(np.argsort(-sc)[:1000].tolist())
+
+
+def test_fused_scoring_matches_layered_gemms(cuda):
+    """The one-launch scoring (weights resident in a two-CTA cluster,
+    activations exchanged through distributed shared memory) gives the
+    per-layer GEMM path's scores."""
+    torch = cuda
+    m = cm.Mlp(1 << 16, seed=11)
+    n = 100_003  # a partial last tile
+    a = m.score_candidates(4242, 17, n, 15, 0, 4, 4, fused=False).cpu().numpy()
+    b = m.score_candidates(4242, 17, n, 15, 0, 4, 4, fused=True).cpu().numpy()
+    assert np.isfinite(b).all()
+    np.testing.assert_allclose(b, a, rtol=1e-4, atol=1e-4 * float(np.abs(a).max()))
+    m.status()
