@@ -474,22 +474,35 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256) mlp_score_fused
     const int tcol = (warp >> 2) * 64;        // this thread's 64 accumulator columns
 
     for (long long tile = blockIdx.x / 2; tile < ntiles; tile += nclusters) {
-        // features of the tile's candidates (K = 64 layout)
-        for (int i = threadIdx.x; i < 128 * 8; i += blockDim.x) {
-            const int row = i >> 3, c = i & 7;
+        // features of the tile's candidates (K = 64 layout): thread `row` < 128
+        // draws its candidate's 15 components (one 64-bit draw per four),
+        // the other threads write the zero columns 24..63
+        if (threadIdx.x < 128) {
+            const int row = threadIdx.x;
             const long long cand = tile * 128 + row;
-            float v[8];
+            float v[24];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int f = 8 * c + j;
-                float x = 0.0f;
-                if (cand < a.n) {
-                    if (f < a.naxes && f < 15) x = 0.25f * (float)candidate_component(a.seed, a.first + cand, f, a.lo, span);
-                    else if (f >= 15 && f < 20) x = (a.family == f - 15) ? 1.0f : 0.0f;
+            for (int f = 0; f < 24; ++f) v[f] = 0.0f;
+            if (cand < a.n) {
+                const long long idx = a.first + cand;
+#pragma unroll
+                for (int w = 0; w < 4; ++w) {
+                    const uint64_t d = splitmix64(a.seed ^ ((uint64_t)idx * 4ull + (uint64_t)w) * 0xD1B54A32D192ED03ull);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int f = 4 * w + q;
+                        if (f < 15 && f < a.naxes)
+                            v[f] = 0.25f * (float)(a.lo + (int)((uint32_t)((d >> (16 * q)) & 0xFFFFull) % (uint32_t)span));
+                    }
                 }
-                v[j] = x;
+                if (a.family >= 0 && a.family < 5) v[15 + a.family] = 1.0f;
             }
-            *(uint4 *)(act + tc::tile_offset(row, 8 * c, kIn)) = pack8(v);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) *(uint4 *)(act + tc::tile_offset(row, 8 * c, kIn)) = pack8(v + 8 * c);
+        } else {
+            const int row = threadIdx.x - 128;
+#pragma unroll
+            for (int c = 3; c < 8; ++c) *(uint4 *)(act + tc::tile_offset(row, 8 * c, kIn)) = make_uint4(0, 0, 0, 0);
         }
         tc::fence_async_smem();
         __syncthreads();
