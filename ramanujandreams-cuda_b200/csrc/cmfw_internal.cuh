@@ -68,67 +68,121 @@ __device__ __forceinline__ int top_axis(uint32_t mask) { return 31 - __clz(mask)
 // dim) already normalised so that their largest |entry| is 1, exactly as
 // the reference's snapshots are.
 // ---------------------------------------------------------------------------
+// Limit candidates of compute_limits (cmf_pfq.cuh:374-460), in its scan
+// order: k = 0 is the primary ratio M[0][r-1] / M[1][r-1]; k >= 1 runs over
+// every (column, i, j), i != j, except the primary. Each candidate pushes an
+// Aitken value and/or a raw ratio, in that order.
+__device__ __forceinline__ int n_limit_candidates(int dim) { return dim * dim * (dim - 1); }
+
+__device__ __forceinline__ void candidate_index(int k, int dim, int &i, int &j, int &cc) {
+    const int c = dim - 1;
+    if (k == 0) {
+        i = 0;
+        j = 1;
+        cc = c;
+        return;
+    }
+    const int per = dim * (dim - 1);
+    const int q0 = c * per;  // the primary's place in the (column, i, j) order
+    const int q = (k - 1 < q0) ? k - 1 : k;
+    cc = q / per;
+    const int r = q % per;
+    i = r / (dim - 1);
+    const int jj = r % (dim - 1);
+    j = jj < i ? jj : jj + 1;
+}
+
+// One candidate: flags bit 0 = Aitken pushed (value *LA), bit 1 = raw pushed (*LR).
+__device__ __forceinline__ int limit_candidate(const double *m1, const double *m2, const double *m3, int dim, int k,
+                                               double *LA, double *LR) {
+    const double DEN_MIN = 1e-280;
+    int i, j, cc;
+    candidate_index(k, dim, i, j, cc);
+    int flags = 0;
+    const double d1 = m1[j * dim + cc], d2 = m2[j * dim + cc], d3 = m3[j * dim + cc];
+    // the primary needs |q| > DEN_MIN, the others |q| >= DEN_MIN (cmf_pfq.cuh:400, 433)
+    if (k == 0 ? (fabs(d1) <= DEN_MIN || fabs(d2) <= DEN_MIN || fabs(d3) <= DEN_MIN)
+               : (fabs(d1) < DEN_MIN || fabs(d2) < DEN_MIN || fabs(d3) < DEN_MIN))
+        return 0;
+    const double r1 = m1[i * dim + cc] / d1, r2 = m2[i * dim + cc] / d2, r3 = m3[i * dim + cc] / d3;
+    if (!isfinite(r1) || !isfinite(r2) || !isfinite(r3)) return 0;
+    const double sc = fmax(1.0, fmax(fabs(r1), fmax(fabs(r2), fabs(r3))));
+    const double den = r1 - 2.0 * r2 + r3;
+    if (fabs(den) > 1e-14 * sc) {
+        const double e = r2 - r3;
+        const double L = r3 - e * e / den;
+        // the primary's Aitken value is kept however small (cmf_pfq.cuh:410, 448)
+        if (isfinite(L) && (k == 0 || fabs(L) > 1e-15)) {
+            *LA = L;
+            flags |= 1;
+        }
+    }
+    if (fabs(r3) > 1e-15) {
+        *LR = r3;
+        flags |= 2;
+    }
+    return flags;
+}
+
+__device__ __forceinline__ int limit_source(int k, int dim, bool aitken) {
+    int i, j, cc;
+    candidate_index(k, dim, i, j, cc);
+    return ((aitken ? 1 : 0) << 12) | (i << 8) | (j << 4) | cc;
+}
+
+// Folds candidate k's pushes into the running selection (first push, first
+// Aitken push, count capped at CMFW_MAX_LIMITS).
+struct LimitScan {
+    int n = 0, src_any = -1, src_aitken = -1;
+    double first_any = 0.0, first_aitken = 0.0;
+    bool have_aitken = false;
+    __device__ __forceinline__ void add(int flags, double LA, double LR, int k, int dim) {
+        if ((flags & 1) && n < CMFW_MAX_LIMITS) {
+            if (n == 0) {
+                first_any = LA;
+                src_any = limit_source(k, dim, true);
+            }
+            if (!have_aitken) {
+                first_aitken = LA;
+                src_aitken = limit_source(k, dim, true);
+                have_aitken = true;
+            }
+            ++n;
+        }
+        if ((flags & 2) && n < CMFW_MAX_LIMITS) {
+            if (n == 0) {
+                first_any = LR;
+                src_any = limit_source(k, dim, false);
+            }
+            ++n;
+        }
+    }
+};
+
+__device__ inline void reduce_tail(const double *m, int dim, const double *ls, double L, cmfw_traj_out &o);
+
 __device__ inline void reduce_snapshots(const double *m, int dim, const double *ls,
                                         cmfw_traj_out &o, int *src_out) {
-    const double DEN_MIN = 1e-280;
+    const int dd = dim * dim;
+    LimitScan sc;
+    const int K = n_limit_candidates(dim);
+    for (int k = 0; k < K; ++k) {
+        double LA = 0.0, LR = 0.0;
+        const int f = limit_candidate(m, m + dd, m + 2 * dd, dim, k, &LA, &LR);
+        if (f) sc.add(f, LA, LR, k, dim);
+    }
+    o.n_limits = sc.n;
+    const double L = sc.have_aitken ? sc.first_aitken : (sc.n > 0 ? sc.first_any : (double)NAN);
+    o.limit = L;
+    *src_out = sc.have_aitken ? sc.src_aitken : (sc.n > 0 ? sc.src_any : -1);
+    reduce_tail(m, dim, ls, L, o);
+}
+
+// p, q, log_scale, precision and delta of the reduction, given the limit.
+__device__ inline void reduce_tail(const double *m, int dim, const double *ls, double L, cmfw_traj_out &o) {
     const int dd = dim * dim;
     const double *m1 = m, *m2 = m + dd, *m3 = m + 2 * dd;
     const int c = dim - 1;
-    int n = 0;
-    double first_aitken = 0.0, first_any = 0.0;
-    int src_aitken = -1, src_any = -1;
-    bool have_aitken = false;
-    // candidate source: (method << 12) | (i << 8) | (j << 4) | column
-    auto push = [&](double L, bool aitken, int i, int j, int cc) {
-        if (n >= CMFW_MAX_LIMITS) return;
-        const int src = ((aitken ? 1 : 0) << 12) | (i << 8) | (j << 4) | cc;
-        if (n == 0) { first_any = L; src_any = src; }
-        if (aitken && !have_aitken) { first_aitken = L; src_aitken = src; have_aitken = true; }
-        ++n;
-    };
-    {
-        double p3 = m3[0 * dim + c], q3 = m3[1 * dim + c];
-        double p2 = m2[0 * dim + c], q2 = m2[1 * dim + c];
-        double p1 = m1[0 * dim + c], q1 = m1[1 * dim + c];
-        if (fabs(q3) > DEN_MIN && fabs(q2) > DEN_MIN && fabs(q1) > DEN_MIN) {
-            double r1 = p1 / q1, r2 = p2 / q2, r3 = p3 / q3;
-            if (isfinite(r1) && isfinite(r2) && isfinite(r3)) {
-                double sc = fmax(1.0, fmax(fabs(r1), fmax(fabs(r2), fabs(r3))));
-                double den = r1 - 2.0 * r2 + r3;
-                if (fabs(den) > 1e-14 * sc) {
-                    double e = r2 - r3;
-                    double L = r3 - e * e / den;
-                    if (isfinite(L)) push(L, true, 0, 1, c);
-                }
-                if (fabs(r3) > 1e-15) push(r3, false, 0, 1, c);
-            }
-        }
-    }
-    for (int cc = 0; cc < dim; ++cc)
-        for (int i = 0; i < dim; ++i)
-            for (int j = 0; j < dim; ++j) {
-                if (i == j) continue;
-                if (cc == c && i == 0 && j == 1) continue;
-                double d1 = m1[j * dim + cc], d2 = m2[j * dim + cc], d3 = m3[j * dim + cc];
-                if (fabs(d1) < DEN_MIN || fabs(d2) < DEN_MIN || fabs(d3) < DEN_MIN) continue;
-                double r1 = m1[i * dim + cc] / d1;
-                double r2 = m2[i * dim + cc] / d2;
-                double r3 = m3[i * dim + cc] / d3;
-                if (!isfinite(r1) || !isfinite(r2) || !isfinite(r3)) continue;
-                double sc = fmax(1.0, fmax(fabs(r1), fmax(fabs(r2), fabs(r3))));
-                double den = r1 - 2.0 * r2 + r3;
-                if (fabs(den) > 1e-14 * sc) {
-                    double e = r2 - r3;
-                    double L = r3 - e * e / den;
-                    if (isfinite(L) && fabs(L) > 1e-15) push(L, true, i, j, cc);
-                }
-                if (fabs(r3) > 1e-15) push(r3, false, i, j, cc);
-            }
-    o.n_limits = n;
-    double L = have_aitken ? first_aitken : (n > 0 ? first_any : (double)NAN);
-    o.limit = L;
-    *src_out = have_aitken ? src_aitken : (n > 0 ? src_any : -1);
-
     double pN = m3[c], qN = m3[dim + c];
     double pNh = m2[c], qNh = m2[dim + c];
     double pN2h = m1[c], qN2h = m1[dim + c];

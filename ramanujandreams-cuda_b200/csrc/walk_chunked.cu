@@ -101,6 +101,53 @@ __global__ void __launch_bounds__(128) walk_prefix_kernel(ChunkArgs C) {
 // 6), 128 above.
 __host__ __device__ constexpr int chunk_threads(int dim) { return dim <= 6 ? 256 : 128; }
 
+// CTA-cooperative products: every task multiplies two DIM x DIM matrices
+// (matrix-exponent form) in the combine arithmetic, one result entry per
+// work item spread over the NT threads; the entries are formed in registers
+// before any is stored (so a task may write over its first operand), and
+// each result is rescaled by a power of two so that its largest entry lies
+// in [1, 2) (per-task maximum through a shared atomic).
+template <class CA>
+struct ProdTask {
+    const typename CA::T *a, *b;
+    typename CA::T *c;
+    int ea, eb;
+    int *ec;
+};
+
+template <int DIM, class CA, int NT, int MAXW>
+__device__ __forceinline__ void par_products(const ProdTask<CA> *tasks, int ntasks, int *pmax) {
+    typedef typename CA::T CT;
+    constexpr int DD = DIM * DIM;
+    CT acc[MAXW];
+#pragma unroll
+    for (int q = 0; q < MAXW; ++q) {
+        const int w = threadIdx.x + q * NT;
+        if (w < ntasks * DD) {
+            const ProdTask<CA> &T = tasks[w / DD];
+            const int e = w % DD, i = e / DIM, j = e % DIM;
+            CT x = CA::mul(T.a[i * DIM], T.b[j]);
+#pragma unroll
+            for (int k = 1; k < DIM; ++k) x = CA::fma(T.a[i * DIM + k], T.b[k * DIM + j], x);
+            acc[q] = x;
+            atomicMax(&pmax[w / DD], CA::hexp(x));
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < MAXW; ++q) {
+        const int w = threadIdx.x + q * NT;
+        if (w < ntasks * DD) {
+            const ProdTask<CA> &T = tasks[w / DD];
+            const int hm = pmax[w / DD];
+            const int be = (hm != 0 && hm < 0x7ff00000) ? (hm >> 20) - 1023 : 0;
+            T.c[w % DD] = CA::scale(acc[q], be);
+            if (w % DD == 0) *T.ec = T.ea + T.eb + be;
+        }
+    }
+    __syncthreads();
+}
+
 // CTAs per cluster of the chunk kernel: a trajectory is walked by one CTA,
 // or by both CTAs of a cluster when the survivors leave enough SMs (chosen
 // on the device from the number of survivors).
@@ -118,9 +165,14 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
     constexpr int PM = (P_ > 0) ? P_ : 8;
     constexpr int QM = (P_ > 0) ? Q_ : 7;
     constexpr int DD = DIM * DIM;
+    constexpr int MAXW = (DD + 1) / 2;          // work items per thread in a tree level
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT *smem = (CT *)smem_raw;                  // NT run products + 6 work matrices
-    int *sexp = (int *)(smem + (NT + 6) * DD);  // NT exponents
+    int *sexp = (int *)(smem + (NT + 6) * DD);  // NT + 6 exponents
+    ProdTask<CA> *tasks = (ProdTask<CA> *)(((uintptr_t)(sexp + NT + 6) + 15) & ~(uintptr_t)15);  // NT / 2
+    int *pmax = (int *)(tasks + NT / 2);        // NT / 2
+    __shared__ int s_ntask, s_fkey, s_ok;
+    __shared__ double s_ls[3];
     // earliest failing lattice step of this CTA's runs, as step * 16 + status
     __shared__ int s_fail;
     cg::cluster_group cluster = cg::this_cluster();
@@ -207,66 +259,121 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
         }
         sexp[tid] = to_matrix_exponent<DIM, A>(m, ex, smem + tid * DD);
         __syncthreads();
-        // in-order tree product of this CTA's runs of each segment
+        // in-order tree product of this CTA's runs of each segment, one
+        // level at a time, every level's products spread over the CTA
         for (int stride = 1; stride < NT; stride <<= 1) {
-            if (active && (lrel % (2 * stride)) == 0 && lrel + stride < ccnt[seg])
-                sexp[tid] = mat_mul_exp<DIM, CA>(smem + tid * DD, sexp[tid], smem + (tid + stride) * DD,
-                                                 sexp[tid + stride], smem + tid * DD);
+            if (tid == 0) s_ntask = 0;
             __syncthreads();
+            if (active && (lrel % (2 * stride)) == 0 && lrel + stride < ccnt[seg]) {
+                const int q = atomicAdd(&s_ntask, 1);
+                tasks[q] = ProdTask<CA>{smem + tid * DD, smem + (tid + stride) * DD, smem + tid * DD, sexp[tid],
+                                        sexp[tid + stride], &sexp[tid]};
+                pmax[q] = 0;
+            }
+            __syncthreads();
+            const int nt = s_ntask;
+            if (nt == 0) break;  // no segment has runs this far apart
+            par_products<DIM, CA, NT, MAXW>(tasks, nt, pmax);
         }
         // every part's products and failure key are final (CTAs that walk
         // alone need no cluster barrier)
         if (NP > 1) cluster.sync();
-        if (active && part == 0 && tid == 0) {
-            // the leader combines the parts in order, then the snapshots
-            int fkey = 0x7fffffff;
-            for (int q = 0; q < NP; ++q) fkey = min(fkey, *cluster.map_shared_rank(&s_fail, crank + q));
-            if (fkey != 0x7fffffff) {
-                write_invalid(W, t, fkey & 15);
+        if (active && part == 0) {
+            // the leader CTA combines the parts in order, forms the snapshots
+            // and reduces them
+            CT *y = smem + NT * DD, *x = y + 3 * DD;
+            int *ye = sexp + NT, *xe = ye + 3;
+            if (tid == 0) {
+                int fkey = 0x7fffffff;
+                for (int q = 0; q < NP; ++q) fkey = min(fkey, *cluster.map_shared_rank(&s_fail, crank + q));
+                s_fkey = fkey;
+                s_ntask = 0;
+                s_ok = 1;
+            }
+            __syncthreads();
+            if (s_fkey != 0x7fffffff) {
+                if (tid == 0) write_invalid(W, t, s_fkey & 15);
             } else {
-                CT *y = smem + NT * DD, *x = y + 3 * DD;
-                int ye[3];
-                for (int k = 0; k < 3; ++k) {
-                    bool have = false;
+                // segment k = first part's product [* second part's product]
+                if (tid < 3) {
+                    const int k = tid;
+                    const CT *pm[2];
+                    int pe[2], np = 0;
                     for (int q = 0; q < NP; ++q) {
                         const int b0q = max(segbase[k], q * NT), b1q = min(segbase[k] + segT[k], (q + 1) * NT);
                         if (b1q <= b0q) continue;
                         const int slot = b0q - q * NT;
-                        CT *pm = cluster.map_shared_rank(smem, crank + q) + slot * DD;
-                        const int pe = *cluster.map_shared_rank(sexp + slot, crank + q);
-                        if (!have) {
-                            for (int i = 0; i < DD; ++i) y[k * DD + i] = pm[i];
-                            ye[k] = pe;
-                            have = true;
-                        } else {
-                            ye[k] = mat_mul_exp<DIM, CA>(y + k * DD, ye[k], pm, pe, y + k * DD);
-                        }
+                        pm[np] = cluster.map_shared_rank(smem, crank + q) + slot * DD;
+                        pe[np] = *cluster.map_shared_rank(sexp + slot, crank + q);
+                        ++np;
+                    }
+                    if (np == 1) {
+                        for (int i = 0; i < DD; ++i) y[k * DD + i] = pm[0][i];
+                        ye[k] = pe[0];
+                    } else {
+                        const int q = atomicAdd(&s_ntask, 1);
+                        tasks[q] = ProdTask<CA>{pm[0], pm[1], y + k * DD, pe[0], pe[1], &ye[k]};
+                        pmax[q] = 0;
                     }
                 }
-                const int e = mat_mul_exp<DIM, CA>((const CT *)C.pre + (size_t)t * DD, C.pre_e[t], y, ye[0], x);
-                const int e1 = mat_mul_exp<DIM, CA>(x, e, y + DD, ye[1], x + DD);
-                const int e2 = mat_mul_exp<DIM, CA>(x + DD, e1, y + 2 * DD, ye[2], x + 2 * DD);
+                __syncthreads();
+                if (s_ntask > 0) par_products<DIM, CA, NT, MAXW>(tasks, s_ntask, pmax);
+                // snapshots: prefix * seg0, then * seg1, then * seg2
+                for (int k = 0; k < 3; ++k) {
+                    if (tid == 0) {
+                        const CT *lhs = k == 0 ? (const CT *)C.pre + (size_t)t * DD : x + (k - 1) * DD;
+                        const int le = k == 0 ? C.pre_e[t] : xe[k - 1];
+                        tasks[0] = ProdTask<CA>{lhs, y + k * DD, x + k * DD, le, ye[k], &xe[k]};
+                        pmax[0] = 0;
+                    }
+                    __syncthreads();
+                    par_products<DIM, CA, NT, MAXW>(tasks, 1, pmax);
+                }
                 double *snap = W.snap + (size_t)t * 3 * DD;
                 int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
-                const int es[3] = {e, e1, e2};
-                bool ok = true;
-                for (int k = 0; k < 3; ++k) {
-                    bool nz = false;
-                    for (int i = 0; i < DD; ++i) {
-                        const double v = CA::to(x[k * DD + i]);
-                        snap[k * DD + i] = v;
-                        ok &= isfinite(v);
-                        nz |= v != 0.0;
-                    }
-                    ok &= nz;
-                    for (int r = 0; r < DIM; ++r) snap_e[k * DIM + r] = es[k];
+                for (int i = tid; i < 3 * DD; i += NT) {
+                    const double v = CA::to(x[i]);
+                    snap[i] = v;
+                    if (!isfinite(v)) atomicAnd(&s_ok, 0);
                 }
-                if (!ok) {
-                    write_invalid(W, t, CMFW_TRAJ_NONFINITE);
+                if (tid < 3 * DIM) snap_e[tid] = xe[tid / DIM];
+                __syncthreads();
+                if (tid < 3) {
+                    bool nz = false;
+                    for (int i = 0; i < DD; ++i) nz |= snap[tid * DD + i] != 0.0;
+                    if (!nz) atomicAnd(&s_ok, 0);
+                }
+                __syncthreads();
+                if (!s_ok) {
+                    if (tid == 0) write_invalid(W, t, CMFW_TRAJ_NONFINITE);
                 } else {
-                    double ls[3];
-                    for (int k = 0; k < 3; ++k) ls[k] = normalise_rows(snap + k * DD, snap_e + k * DIM, DIM, 0.0);
-                    finish_valid(W, t, snap, DIM, ls);
+                    if (tid < 3) s_ls[tid] = normalise_rows(snap + tid * DD, snap_e + tid * DIM, DIM, 0.0);
+                    __syncthreads();
+                    // limit candidates in parallel, then the in-order selection
+                    const int K = n_limit_candidates(DIM);
+                    int *cf = (int *)smem;                     // run products are no longer needed
+                    double *cla = (double *)(smem) + K, *clr = cla + K;
+                    for (int k = tid; k < K; k += NT) {
+                        double LA = 0.0, LR = 0.0;
+                        cf[k] = limit_candidate(snap, snap + DD, snap + 2 * DD, DIM, k, &LA, &LR);
+                        cla[k] = LA;
+                        clr[k] = LR;
+                    }
+                    __syncthreads();
+                    if (tid == 0) {
+                        LimitScan scn;
+                        for (int k = 0; k < K; ++k)
+                            if (cf[k]) scn.add(cf[k], cla[k], clr[k], k, DIM);
+                        cmfw_traj_out o;
+                        o.valid = 1;
+                        o.n_limits = scn.n;
+                        o.limit = scn.have_aitken ? scn.first_aitken : (scn.n > 0 ? scn.first_any : (double)NAN);
+                        reduce_tail(snap, DIM, s_ls, o.limit, o);
+                        W.out[t] = o;
+                        if (W.status) W.status[t] = CMFW_TRAJ_OK;
+                        if (W.limit_src)
+                            W.limit_src[t] = scn.have_aitken ? scn.src_aitken : (scn.n > 0 ? scn.src_any : -1);
+                    }
                 }
             }
         }
@@ -326,7 +433,8 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     C.count = (int *)p;
     C.prefix_steps = prefix_steps;
     const int NT = chunk_threads(dim);
-    const size_t shmem = (size_t)(NT + 6) * dim * dim * sizeof(typename A::Combine::T) + NT * sizeof(int);
+    const size_t shmem = (size_t)(NT + 6) * dim * dim * sizeof(typename A::Combine::T) + (NT + 6) * sizeof(int) + 16 +
+                         (size_t)(NT / 2) * (sizeof(ProdTask<typename A::Combine>) + sizeof(int));
     cudaError_t e = cudaFuncSetAttribute((const void *)k.chunk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shmem);
     if (e != cudaSuccess) return e;
