@@ -156,7 +156,7 @@ cmfw_status cmfw_walk_f64(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_
  * which every GPU that loads the library holds until the process exits. The
  * caller passes device inputs and outputs as for cmfw_walk_f64.
  *  - Capacity: cmfw_walk_workspace_bytes(desc, n_traj) must not exceed
- *    CMFW_NOALLOC_SCRATCH_BYTES (about 38,000 trajectories at rank 5, 15,000
+ *    CMFW_NOALLOC_SCRATCH_BYTES (about 50,000 trajectories at rank 5, 20,000
  *    at rank 8); a larger batch returns CMFW_EINVAL, and the caller splits it.
  *  - Set-up: the first call on a device looks up the array's device address
  *    (cudaGetSymbolAddress) with that device current; make that first call

@@ -126,7 +126,7 @@ cudaError_t host_staging(int n, cmfw_traj_in **in, cmfw_traj_out **out) {
 }
 
 // Snapshot matrices and row exponents of every trajectory, followed by the
-// chunked walk's prefix products, survivor list and counter.
+// chunked walk's survivor list and counter.
 size_t snapshot_bytes(int dim, int n) {
     return align256((size_t)n * 3 * dim * dim * sizeof(double)) + align256((size_t)n * 3 * dim * sizeof(int)) +
            chunk_scratch_bytes(dim, n);

@@ -5,25 +5,30 @@
 // into chunks walked independently and multiplied back together in order.
 // Two kernels:
 //
-//  1. prefix: one thread per trajectory walks the first S lattice steps
-//     (S = min(prefix_steps, N-2h-1)). Most trajectories that fail, fail
-//     here (zeta starts hit a singular lead coefficient on their first y+
-//     step), and leave after a handful of steps. Survivors store their
-//     prefix product and append their index to a list.
+//  1. filter: one thread per trajectory walks the first S lattice steps in
+//     plain FP64 (S = min(prefix_steps, N-2h-1)) and keeps nothing but the
+//     verdict: a trajectory that fails there is written invalid with its
+//     status, a survivor appends its index to a list. Most trajectories
+//     that fail, fail here (zeta starts hit a singular lead coefficient on
+//     their first y+ step). The step's singularity tests use the FP64
+//     column, denominators and solve, which every arithmetic forms the same
+//     way, so the verdict is the run arithmetic's.
 //  2. chunk: clusters of 2 CTAs of NT threads (256 up to rank 6, else 128)
 //     on a persistent grid that strides over the survivor list; each
 //     survivor is walked by one CTA, or by both CTAs of a cluster when there
 //     are fewer survivors than half the CTAs (the parts are multiplied in
-//     order through distributed shared memory). The remaining steps form three segments [S+1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the snapshot
-//     depths are segment ends); each thread walks a contiguous run of lattice
-//     steps of one segment with the same registers-only step as the
-//     sequential kernel, the runs of a segment are multiplied in order by a
-//     shared-memory tree, and thread 0 forms the three snapshots
-//     prefix * seg0, * seg1, * seg2 and reduces them.
+//     order through distributed shared memory). Steps 1..N form three
+//     segments [1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the snapshot depths are
+//     segment ends); each thread walks a contiguous run of lattice steps of
+//     one segment with the same registers-only step as the sequential
+//     kernel, the runs of a segment are multiplied in order by a
+//     shared-memory tree, and the leader CTA forms the three snapshots
+//     seg0, seg0 * seg1, seg0 * seg1 * seg2 and reduces them.
 //
 // The latency of one trajectory drops from N lattice steps to about
-// (N - S) / NT + log2 NT matrix products; the total arithmetic is that of
-// the sequential walk plus NT - 1 dense rank^3 products.
+// N / (NP * NT) lattice steps + log2 NT matrix products; the total
+// arithmetic is that of the sequential walk plus NP * NT - 1 dense rank^3
+// products.
 //
 // Accuracy. Multiplying runs together is a different association of the
 // same matrix product. A run started from the identity can pass through
@@ -48,16 +53,14 @@ namespace cmfw {
 
 struct ChunkArgs {
     WalkArgs w;
-    void *pre;     // n_traj * DIM * DIM prefix products (matrix exponent form,
-                   // in the combine arithmetic: double or double-double)
-    int *pre_e;    // n_traj
     int *list;     // n_traj survivor indices
     int *count;    // survivors
     int prefix_steps;
 };
 
-template <int P_, int Q_, int DIM, class A>
+template <int P_, int Q_, int DIM>
 __global__ void __launch_bounds__(128) walk_prefix_kernel(ChunkArgs C) {
+    typedef ArithF64 A;
     typedef typename A::T T;
     const WalkArgs &W = C.w;
     constexpr int NAX = (P_ > 0) ? (P_ + Q_) : CMFW_MAX_AXES;
@@ -92,8 +95,6 @@ __global__ void __launch_bounds__(128) walk_prefix_kernel(ChunkArgs C) {
         if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
         if (st != CMFW_TRAJ_OK) { write_invalid(W, t, st); return; }
     }
-    typedef typename A::Combine::T CT;
-    C.pre_e[t] = to_matrix_exponent<DIM, A>(m, ex, (CT *)C.pre + (size_t)t * DIM * DIM);
     C.list[atomicAdd(C.count, 1)] = t;
 }
 
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
 
     // segments of lattice steps and the runs (global index g over the NP
     // CTAs) that cover them; the same for every trajectory of the launch
-    const int S = min(C.prefix_steps, W.N - 2 * W.h - 1);
+    const int S = 0;
     const int cp1 = W.N - 2 * W.h, cp2 = W.N - W.h;
     const int L0 = cp1 - S, L1 = W.h, L2 = W.h;
     const int rest = W.N - S;
@@ -318,12 +319,13 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
                 }
                 __syncthreads();
                 if (s_ntask > 0) par_products<DIM, CA, NT, MAXW>(tasks, s_ntask, pmax);
-                // snapshots: prefix * seg0, then * seg1, then * seg2
-                for (int k = 0; k < 3; ++k) {
+                // snapshots: seg0, then * seg1, then * seg2
+                for (int i = tid; i < DD; i += NT) x[i] = y[i];
+                if (tid == 0) xe[0] = ye[0];
+                __syncthreads();
+                for (int k = 1; k < 3; ++k) {
                     if (tid == 0) {
-                        const CT *lhs = k == 0 ? (const CT *)C.pre + (size_t)t * DD : x + (k - 1) * DD;
-                        const int le = k == 0 ? C.pre_e[t] : xe[k - 1];
-                        tasks[0] = ProdTask<CA>{lhs, y + k * DD, x + k * DD, le, ye[k], &xe[k]};
+                        tasks[0] = ProdTask<CA>{x + (k - 1) * DD, y + k * DD, x + k * DD, xe[k - 1], ye[k], &xe[k]};
                         pmax[0] = 0;
                     }
                     __syncthreads();
@@ -396,11 +398,11 @@ template <class A>
 static ChunkPick<A> pick_chunk(int p, int q, int dim) {
 #define CMFW_CASE(P, Q, D)                                                                        \
     if (p == P && q == Q && dim == D)                                                             \
-        return ChunkPick<A>{walk_prefix_kernel<P, Q, D, A>, walk_chunk_kernel<P, Q, D, A>, D};
+        return ChunkPick<A>{walk_prefix_kernel<P, Q, D>, walk_chunk_kernel<P, Q, D, A>, D};
     CMFW_FAMILY_CASES
 #undef CMFW_CASE
 #define CMFW_GEN(D) \
-    case D: return ChunkPick<A>{walk_prefix_kernel<0, 0, D, A>, walk_chunk_kernel<0, 0, D, A>, D};
+    case D: return ChunkPick<A>{walk_prefix_kernel<0, 0, D>, walk_chunk_kernel<0, 0, D, A>, D};
     switch (dim) {
         CMFW_GEN(2) CMFW_GEN(3) CMFW_GEN(4) CMFW_GEN(5) CMFW_GEN(6) CMFW_GEN(7) CMFW_GEN(8)
     }
@@ -408,11 +410,11 @@ static ChunkPick<A> pick_chunk(int p, int q, int dim) {
     return ChunkPick<A>{nullptr, nullptr, 0};
 }
 
-// Prefix products are stored in the combine arithmetic: at most 16 bytes
-// (double-double) per entry.
+// Survivor list and counter.
 size_t chunk_scratch_bytes(int dim, int n) {
+    (void)dim;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    return al((size_t)n * dim * dim * 16) + al((size_t)n * sizeof(int)) * 2 + 256;
+    return al((size_t)n * sizeof(int)) + 256;
 }
 
 template <class A>
@@ -424,10 +426,6 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     ChunkArgs C;
     C.w = W;
     char *p = (char *)scratch;
-    C.pre = (void *)p;
-    p += al((size_t)n * dim * dim * 16);
-    C.pre_e = (int *)p;
-    p += al((size_t)n * sizeof(int));
     C.list = (int *)p;
     p += al((size_t)n * sizeof(int));
     C.count = (int *)p;

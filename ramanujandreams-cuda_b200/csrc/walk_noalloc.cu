@@ -5,7 +5,7 @@
 // memory all comes from another allocator's pool (a framework's caching
 // allocator that accounts for every byte), and code that must not
 // synchronise the device mid-run, which a first cudaMalloc or cudaFree may
-// do. The walk's scratch (snapshot matrices, prefix products, survivor list
+// do. The walk's scratch (snapshot matrices, row exponents, survivor list
 // and counter) lives in g_noalloc_scratch below; inputs and outputs remain
 // the caller's.
 //
