@@ -379,7 +379,9 @@ def main_mixed(args):
     U{1..10}, directions U{0..3} (not all zero), N log-uniform in 200..5000,
     h = 50, walked in one CUDA-graph launch (sort + per-descriptor persistent
     kernels). Reports traj/s of the baseline tiles (one thread per sorted
-    trajectory, 256-thread CTAs), the default tiles and the autotuned tiles."""
+    trajectory, 256-thread CTAs), the persistent queues (default tiles) with
+    and without the singularity prescan, and the autotuned tiles (per
+    descriptor the fastest of plain grids and queues)."""
     import torch
     import cmfw
     import cmfw.workloads as wl
@@ -396,7 +398,11 @@ def main_mixed(args):
     tuned = b.autotune()
     t_tune = time.perf_counter() - t0
     res = {}
-    for name, tuning in (("baseline_256", cmfw.baseline_tuning()), ("default", None), ("autotuned", tuned)):
+    scan = cmfw.MixedTuning()
+    scan.persistent = 1
+    scan.prescan = 1
+    for name, tuning in (("baseline_256", cmfw.baseline_tuning()), ("default", None),
+                         ("persistent_prescan", scan), ("autotuned", tuned)):
         b.capture(tuning)
         b.replay()
         torch.cuda.synchronize()

@@ -229,21 +229,25 @@ typedef struct {
 } cmfw_mixed_item;
 typedef struct {
     int block_size;  /* threads per CTA: 64, 128 or 256 */
-    int grab;        /* trajectories a warp takes per queue access (multiple of 32) */
+    int grab;        /* trajectories a warp takes per queue access (multiple of
+                        32); 0 = a plain grid, one sorted trajectory per thread */
     int ctas_per_sm; /* resident CTAs per SM, 0 = as many as fit */
 } cmfw_mixed_tile;
 typedef struct {
     int persistent; /* 1: cost-sorted queues (tiles below); 0: the baseline, one
                        thread per sorted trajectory in 256-thread CTAs */
     cmfw_mixed_tile tile[CMFW_MAX_MIXED_DESCS];
+    int prescan;    /* with persistent: follow every trajectory through its N
+                       steps with the position-only singularity tests first
+                       and walk only the survivors */
 } cmfw_mixed_tuning;
 size_t cmfw_mixed_workspace_bytes(int n_traj, int n_descs);
-/* tuning NULL = persistent, 128 threads, grab 32, full occupancy. */
+/* tuning NULL = persistent, 128 threads, grab 32, full occupancy, no prescan. */
 cmfw_status cmfw_walk_mixed(const cmfw_desc *descs, int n_descs, const cmfw_traj_in *d_in,
                             const cmfw_mixed_item *d_items, cmfw_traj_out *d_out, int n_traj, int h,
                             int variant, const cmfw_mixed_tuning *tuning, const cmfw_launch *launch,
                             void *stream);
-/* Autotuner: per descriptor, times every (block 64/128/256) x (grab 32/64)
+/* Autotuner: per descriptor, times every (block 64/128/256) x (grab 0/32/64)
  * on a strided sample of up to `sample` (0 = 65536) of that descriptor's
  * cost-sorted trajectories and keeps the fastest. Synchronises the stream;
  * writes scratch results into d_out. */

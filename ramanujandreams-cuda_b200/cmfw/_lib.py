@@ -78,7 +78,7 @@ class MixedTile(ctypes.Structure):
 
 class MixedTuning(ctypes.Structure):
     """cmfw_mixed_tuning."""
-    _fields_ = [("persistent", ctypes.c_int), ("tile", MixedTile * 16)]
+    _fields_ = [("persistent", ctypes.c_int), ("tile", MixedTile * 16), ("prescan", ctypes.c_int)]
 
 
 _lib = None

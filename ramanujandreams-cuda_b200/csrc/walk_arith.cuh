@@ -226,15 +226,26 @@ struct StepConst {
     double lead_scale_fixed;   // max(1, |1 - z|)
 };
 
-// One axis step: M <- M (I + C/a) or M (I + C/a)^-1, then the position
-// moves by `up ? +1 : -1` along `axis`. Returns a cmfw_traj_status.
-template <int DIM, int NAX, int PM, int QM, class A>
-__device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], double (&pos)[NAX],
-                                         int axis, bool up, const StepConst &K) {
-    typedef typename A::T T;
+// The position-only part of an axis step (cmf_pfq.cuh:146-181, 186-225):
+// the companion column -d/lead, 1/a and, for inverse steps, the
+// row-independent beta vector and scalar solve, with the reference's
+// singularity tests (cmf_pfq.cuh:173, 193, 225). None of it depends on the
+// walk matrix. With FULL = false only what the tests need is formed (the
+// column of a forward step is skipped). Returns a cmfw_traj_status.
+template <int DIM>
+struct StepMatrix {
+    double col[DIM], be[DIM];
+    double inva, sd;
+    bool inverse;
+};
+
+template <bool FULL, int DIM, int NAX, int PM, int QM>
+__device__ __forceinline__ int step_matrix(const double (&pos)[NAX], int axis, bool up, const StepConst &K,
+                                           StepMatrix<DIM> &S) {
     const int P = K.P, Q = K.Q;
     const bool is_x = axis < P;
     const bool inverse = is_x ? !up : up;
+    S.inverse = inverse;
     // evaluation point: x- steps evaluate at x-1, y+ steps at y+1
     const double dlt = inverse ? (is_x ? -1.0 : 1.0) : 0.0;
     double pa = 0.0;
@@ -264,42 +275,57 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)
     }
     if (lead_bad) return CMFW_TRAJ_SINGULAR_LEAD;
     if (!isfinite(denom) || fabs(denom) <= 64.0 * CMFW_EPS64) return CMFW_TRAJ_SINGULAR_DENOM;
+    if (!FULL && !inverse) return CMFW_TRAJ_OK;
     const double il = 1.0 / lead;
     const double inva = 1.0 / denom;
+    S.inva = inva;
     // col = -d / lead: the reciprocal product plus one residual correction
     // (the reference divides, cmf_pfq.cuh:177)
-    double col[DIM];
 #pragma unroll
     for (int i = 0; i < DIM; ++i) {
         const double c0 = __dmul_rn(-d[i], il);
-        col[i] = __fma_rn(__fma_rn(-c0, lead, -d[i]), il, c0);
+        S.col[i] = __fma_rn(__fma_rn(-c0, lead, -d[i]), il, c0);
     }
+    if (inverse) {
+        // back-substitution in t = out[DIM-1] (cmf_pfq.cuh:207-235); beta and
+        // the scalar solve do not depend on the row
+        S.be[DIM - 1] = 1.0;
+#pragma unroll
+        for (int j = DIM - 2; j >= 0; --j) S.be[j] = -S.be[j + 1] * inva;
+        double db = S.be[0] * S.col[0];
+#pragma unroll
+        for (int k = 1; k < DIM; ++k) db = __fma_rn(S.be[k], S.col[k], db);
+        const double sd = __fma_rn(db, inva, 1.0);
+        const double ss = fmax(1.0, fabs(db * inva));
+        if (!isfinite(sd) || fabs(sd) <= 128.0 * CMFW_EPS64 * ss) return CMFW_TRAJ_SINGULAR_SOLVE;
+        S.sd = sd;
+    }
+    return CMFW_TRAJ_OK;
+}
 
-    if (!inverse) {
+// One axis step: M <- M (I + C/a) or M (I + C/a)^-1, then the position
+// moves by `up ? +1 : -1` along `axis`. Returns a cmfw_traj_status.
+template <int DIM, int NAX, int PM, int QM, class A>
+__device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], double (&pos)[NAX],
+                                         int axis, bool up, const StepConst &K) {
+    typedef typename A::T T;
+    StepMatrix<DIM> S;
+    const int st = step_matrix<true, DIM, NAX, PM, QM>(pos, axis, up, K, S);
+    if (st != CMFW_TRAJ_OK) return st;
+    const double inva = S.inva;
+    if (!S.inverse) {
         // out[j] = m[j] + m[j+1]/a, last += (m . col)/a
 #pragma unroll
         for (int r = 0; r < DIM; ++r) {
-            T dot = A::mul_s(m[r][0], col[0]);
+            T dot = A::mul_s(m[r][0], S.col[0]);
 #pragma unroll
-            for (int k = 1; k < DIM; ++k) dot = A::fma_s(m[r][k], col[k], dot);
+            for (int k = 1; k < DIM; ++k) dot = A::fma_s(m[r][k], S.col[k], dot);
 #pragma unroll
             for (int j = 0; j < DIM - 1; ++j) m[r][j] = A::fma_s(m[r][j + 1], inva, m[r][j]);
             m[r][DIM - 1] = A::fma_s(dot, inva, m[r][DIM - 1]);
         }
     } else {
-        // back-substitution in t = out[DIM-1] (cmf_pfq.cuh:207-235); beta and
-        // the scalar solve do not depend on the row and are formed in FP64
-        double be[DIM];
-        be[DIM - 1] = 1.0;
-#pragma unroll
-        for (int j = DIM - 2; j >= 0; --j) be[j] = -be[j + 1] * inva;
-        double db = be[0] * col[0];
-#pragma unroll
-        for (int k = 1; k < DIM; ++k) db = __fma_rn(be[k], col[k], db);
-        const double sd = __fma_rn(db, inva, 1.0);
-        const double ss = fmax(1.0, fabs(db * inva));
-        if (!isfinite(sd) || fabs(sd) <= 128.0 * CMFW_EPS64 * ss) return CMFW_TRAJ_SINGULAR_SOLVE;
-        const double isd = 1.0 / sd;
+        const double isd = 1.0 / S.sd;
         const double ninva = -inva;
 #pragma unroll
         for (int r = 0; r < DIM; ++r) {
@@ -308,12 +334,12 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)
             al[DIM - 2] = m[r][DIM - 2];
 #pragma unroll
             for (int j = DIM - 3; j >= 0; --j) al[j] = A::fma_s(al[j + 1], ninva, m[r][j]);
-            T da = A::mul_s(al[0], col[0]);
+            T da = A::mul_s(al[0], S.col[0]);
 #pragma unroll
-            for (int k = 1; k < DIM - 1; ++k) da = A::fma_s(al[k], col[k], da);
-            const T tt = A::div_s(A::fma_s(da, ninva, m[r][DIM - 1]), sd, isd);
+            for (int k = 1; k < DIM - 1; ++k) da = A::fma_s(al[k], S.col[k], da);
+            const T tt = A::div_s(A::fma_s(da, ninva, m[r][DIM - 1]), S.sd, isd);
 #pragma unroll
-            for (int j = 0; j < DIM; ++j) m[r][j] = A::fma_s(tt, be[j], al[j]);
+            for (int j = 0; j < DIM; ++j) m[r][j] = A::fma_s(tt, S.be[j], al[j]);
         }
     }
 #pragma unroll
@@ -336,6 +362,27 @@ __device__ __forceinline__ int lattice_step(typename A::T (&m)[DIM][DIM], int (&
             mask &= ~(1u << axis);
             const int st = axis_step<DIM, NAX, PM, QM, A>(m, ex, pos, axis, !((neg >> axis) & 1u), K);
             if (st != CMFW_TRAJ_OK) return st;
+        }
+    }
+    return CMFW_TRAJ_OK;
+}
+
+// The singularity tests of one lattice displacement without the matrix
+// update (the steps that decide validity depend on the position only).
+template <int DIM, int NAX, int PM, int QM>
+__device__ __forceinline__ int lattice_step_tests(double (&pos)[NAX], const int (&absd)[NAX], uint32_t neg,
+                                                  int maxabs, const StepConst &K) {
+    for (int level = maxabs; level >= 1; --level) {
+        uint32_t mask = level_mask<NAX>(absd, level);
+        while (mask) {
+            const int axis = top_axis(mask);
+            mask &= ~(1u << axis);
+            const bool up = !((neg >> axis) & 1u);
+            StepMatrix<DIM> S;
+            const int st = step_matrix<false, DIM, NAX, PM, QM>(pos, axis, up, K, S);
+            if (st != CMFW_TRAJ_OK) return st;
+#pragma unroll
+            for (int a = 0; a < NAX; ++a) pos[a] += (a == axis) ? (up ? 1.0 : -1.0) : 0.0;
         }
     }
     return CMFW_TRAJ_OK;

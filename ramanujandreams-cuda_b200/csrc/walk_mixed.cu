@@ -16,8 +16,15 @@
 //  4. walk:    per family, a persistent kernel (grid = SMs x resident CTAs)
 //              whose warps take `grab` consecutive sorted trajectories at a
 //              time from the family's queue (an atomic counter): neighbours
-//              in a warp have similar depth, and the longest walks start
-//              first, so the tail is short.
+//              in a warp have similar depth and the longest walks start
+//              first, so the tail is short; or a plain grid of one
+//              trajectory per thread in cost order (tile grab 0).
+//  Optional (tuning->prescan): before 4, a persistent scan follows each
+//  trajectory through its N steps with the position-only singularity tests
+//  (no matrix), writes the failures' results at once and compacts the
+//  survivors for the walk. On the benchmark mix it costs more than it saves
+//  (the tests are over half a step's work at small ranks, and survivors pay
+//  for both), so it is off by default.
 //
 // The walk of one trajectory is the sequential kernel's (walk_seq.cuh) in the
 // launch's arithmetic (FP64, or float-float on the FP32 pipe with the FP64
@@ -44,6 +51,9 @@ struct MixedArgs {
     const int *order;              // trajectory indices, sorted
     const int *begin;              // n_descs + 1 offsets of each family in order
     int *next;                     // n_descs queue heads (start at zero)
+    const int *seg_len;            // optional: family lengths (else begin[f+1] - begin[f])
+    int *alive;                    // survivors of the scan, at each family's offset
+    int *alive_count;              // n_descs
     int grab;                      // trajectories a warp takes per queue access
     cmfw_desc descs[CMFW_MAX_MIXED_DESCS];
     int n_descs;
@@ -117,7 +127,7 @@ __global__ void __launch_bounds__(256) walk_mixed_kernel(MixedArgs M, int fam, i
     double snap[3 * DIM * DIM];
     int snap_e[3 * DIM];
     const int lo = M.begin[fam];
-    const int len = M.begin[fam + 1] - lo;
+    const int len = M.seg_len ? M.seg_len[fam] : M.begin[fam + 1] - lo;
     if (!persistent) {
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i < len) {
@@ -140,6 +150,54 @@ __global__ void __launch_bounds__(256) walk_mixed_kernel(MixedArgs M, int fam, i
             }
         }
     }
+}
+
+// The singularity scan of family `fam`: each trajectory of its sorted
+// segment is followed through steps 1..N with the position-only tests; a
+// failure is written as the trajectory's result right away, a survivor is
+// appended to the family's part of M.alive for the walk.
+template <int P_, int Q_, int DIM>
+__global__ void __launch_bounds__(256) scan_mixed_kernel(MixedArgs M, int fam) {
+    WalkArgs W = M.w;
+    W.p = M.descs[fam].p;
+    W.q = M.descs[fam].q;
+    W.dim = M.descs[fam].rank;
+    W.z = M.descs[fam].z;
+    const int lo = M.begin[fam];
+    const int len = M.begin[fam + 1] - lo;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&M.next[fam], 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= len) break;
+        const int i = base + lane;
+        if (i < len) {
+            const int t = M.order[lo + i];
+            const int st = scan_failure<P_, Q_, DIM>(W, t, M.items[t].N);
+            if (st != CMFW_TRAJ_OK) write_invalid(W, t, st);
+            else M.alive[lo + atomicAdd(&M.alive_count[fam], 1)] = t;
+        }
+    }
+}
+
+typedef void (*scan_kernel_t)(MixedArgs, int);
+
+static scan_kernel_t pick_scan(int p, int q, int dim) {
+#define CMFW_CASE(P, Q, D) \
+    if (p == P && q == Q && dim == D) return scan_mixed_kernel<P, Q, D>;
+    CMFW_FAMILY_CASES
+#undef CMFW_CASE
+    switch (dim) {
+        case 2: return scan_mixed_kernel<0, 0, 2>;
+        case 3: return scan_mixed_kernel<0, 0, 3>;
+        case 4: return scan_mixed_kernel<0, 0, 4>;
+        case 5: return scan_mixed_kernel<0, 0, 5>;
+        case 6: return scan_mixed_kernel<0, 0, 6>;
+        case 7: return scan_mixed_kernel<0, 0, 7>;
+        case 8: return scan_mixed_kernel<0, 0, 8>;
+    }
+    return nullptr;
 }
 
 typedef void (*mixed_kernel_t)(MixedArgs, int, int);
@@ -170,16 +228,19 @@ static mixed_kernel_t pick_mixed_variant(int variant, const cmfw_desc &d) {
 // Workspace: histogram and cursors (n_descs * 64 ints each), begin
 // (n_descs + 1), queue heads (n_descs), keys (n), order (n).
 struct MixedLayout {
-    int *hist, *cursor, *begin, *next, *keys, *order;
+    int *hist, *cursor, *begin, *next, *next2, *alive_count, *keys, *order, *alive;
     size_t small_bytes;  // what must be zeroed before each walk
 };
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+static size_t mixed_small_bytes() {
+    return al256(sizeof(int) * (2 * CMFW_MAX_MIXED_DESCS * kCostBuckets + 4 * (CMFW_MAX_MIXED_DESCS + 1)));
+}
+
 static size_t mixed_ws_bytes(int n, int n_descs) {
     (void)n_descs;
-    return al256(sizeof(int) * (2 * CMFW_MAX_MIXED_DESCS * kCostBuckets + 2 * (CMFW_MAX_MIXED_DESCS + 1))) +
-           2 * al256(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    return mixed_small_bytes() + 3 * al256(sizeof(int) * (size_t)(n > 0 ? n : 1));
 }
 
 static MixedLayout mixed_layout(void *ws, int n) {
@@ -189,10 +250,14 @@ static MixedLayout mixed_layout(void *ws, int n) {
     L.cursor = p + CMFW_MAX_MIXED_DESCS * kCostBuckets;
     L.begin = L.cursor + CMFW_MAX_MIXED_DESCS * kCostBuckets;
     L.next = L.begin + CMFW_MAX_MIXED_DESCS + 1;
-    L.small_bytes = al256(sizeof(int) * (2 * CMFW_MAX_MIXED_DESCS * kCostBuckets + 2 * (CMFW_MAX_MIXED_DESCS + 1)));
+    L.next2 = L.next + CMFW_MAX_MIXED_DESCS + 1;
+    L.alive_count = L.next2 + CMFW_MAX_MIXED_DESCS + 1;
+    L.small_bytes = mixed_small_bytes();
+    const size_t arr = al256(sizeof(int) * (size_t)(n > 0 ? n : 1));
     char *q = (char *)ws + L.small_bytes;
     L.keys = (int *)q;
-    L.order = (int *)(q + al256(sizeof(int) * (size_t)(n > 0 ? n : 1)));
+    L.order = (int *)(q + arr);
+    L.alive = (int *)(q + 2 * arr);
     return L;
 }
 
@@ -227,18 +292,21 @@ static cudaError_t enqueue_sort(const MixedArgs &M, const MixedLayout &L, cudaSt
     return cudaGetLastError();
 }
 
+// One family's walk: a plain grid of one trajectory per thread (baseline,
+// or a tile with grab 0), or the persistent queue of the tile.
 static cudaError_t enqueue_family(const MixedArgs &M, int f, int variant, const cmfw_mixed_tile &tile,
                                   int persistent, cudaStream_t s) {
     mixed_kernel_t k = pick_mixed_variant(variant, M.descs[f]);
     if (!k) return cudaErrorInvalidValue;
     MixedArgs Mf = M;
-    if (!persistent) {
-        const int n = M.w.n_traj;
-        k<<<(n + 255) / 256, 256, 0, s>>>(Mf, f, 0);
-        return cudaGetLastError();
-    }
     int block = tile.block_size;
     if (block != 64 && block != 128 && block != 256) block = 128;
+    if (!persistent || tile.grab == 0) {
+        if (!persistent) block = 256;
+        const int n = M.w.n_traj;
+        k<<<(n + block - 1) / block, block, 0, s>>>(Mf, f, 0);
+        return cudaGetLastError();
+    }
     Mf.grab = (tile.grab >= 32 && tile.grab % 32 == 0) ? tile.grab : 32;
     int per_sm = resident_ctas(k, block);
     if (tile.ctas_per_sm > 0 && tile.ctas_per_sm < per_sm) per_sm = tile.ctas_per_sm;
@@ -276,17 +344,42 @@ static MixedArgs make_args(const cmfw_desc *descs, int n_descs, const cmfw_traj_
     M.order = L.order;
     M.begin = L.begin;
     M.next = L.next;
+    M.seg_len = nullptr;
+    M.alive = L.alive;
+    M.alive_count = L.alive_count;
     M.grab = 32;
     for (int i = 0; i < n_descs; ++i) M.descs[i] = descs[i];
     M.n_descs = n_descs;
     return M;
 }
 
+// Per family: the singularity scan (persistent, cost-sorted queue), then the
+// walk of its survivors only (tuning->prescan), or the walk of every
+// trajectory.
 static cudaError_t enqueue_mixed(const MixedArgs &M, const MixedLayout &L, int variant,
                                  const cmfw_mixed_tuning &tune, cudaStream_t s) {
     cudaError_t e = enqueue_sort(M, L, s);
-    for (int f = 0; f < M.n_descs && e == cudaSuccess; ++f)
-        e = enqueue_family(M, f, variant, tune.tile[f], tune.persistent, s);
+    const bool prescan = tune.persistent && tune.prescan;
+    for (int f = 0; f < M.n_descs && e == cudaSuccess; ++f) {
+        if (!prescan) {
+            e = enqueue_family(M, f, variant, tune.tile[f], tune.persistent, s);
+            continue;
+        }
+        scan_kernel_t k = pick_scan(M.descs[f].p, M.descs[f].q, M.descs[f].rank);
+        if (!k) return cudaErrorInvalidValue;
+        MixedArgs Ms = M;
+        Ms.next = L.next2;
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)k, 256, 0) != cudaSuccess || nb < 1)
+            nb = 1;
+        k<<<sm_count() * nb, 256, 0, s>>>(Ms, f);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) break;
+        MixedArgs Mw = M;
+        Mw.order = L.alive;
+        Mw.seg_len = L.alive_count;
+        e = enqueue_family(Mw, f, variant, tune.tile[f], 1, s);
+    }
     return e;
 }
 
@@ -306,6 +399,7 @@ cmfw_mixed_tuning default_tuning(int n_descs) {
     cmfw_mixed_tuning t;
     memset(&t, 0, sizeof(t));
     t.persistent = 1;
+    t.prescan = 0;
     for (int i = 0; i < n_descs && i < CMFW_MAX_MIXED_DESCS; ++i) default_tile(t.tile[i]);
     return t;
 }
@@ -374,7 +468,7 @@ cmfw_status cmfw_mixed_autotune(const cmfw_desc *descs, int n_descs, const cmfw_
     if (e == cudaSuccess) e = cudaEventCreate(&a);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     const int blocks[3] = {64, 128, 256};
-    const int grabs[2] = {32, 64};
+    const int grabs[3] = {0, 32, 64};  // 0: plain grid, one trajectory per thread
     for (int f = 0; f < n_descs && e == cudaSuccess; ++f) {
         const int len = begin[f + 1] - begin[f];
         if (len <= 0) continue;
@@ -391,7 +485,7 @@ cmfw_status cmfw_mixed_autotune(const cmfw_desc *descs, int n_descs, const cmfw_
         Ms.next = d_snext;
         float best = 1e30f;
         for (int bi = 0; bi < 3 && e == cudaSuccess; ++bi)
-            for (int gi = 0; gi < 2 && e == cudaSuccess; ++gi) {
+            for (int gi = 0; gi < 3 && e == cudaSuccess; ++gi) {
                 cmfw_mixed_tile tile;
                 tile.block_size = blocks[bi];
                 tile.grab = grabs[gi];

@@ -70,3 +70,37 @@ __device__ __forceinline__ void walk_seq_one(const WalkArgs &W, int t, int N, do
 }
 
 }  // namespace cmfw
+
+namespace cmfw {
+
+// Whether trajectory t survives steps 1..N, decided from the singularity
+// tests alone (step_matrix: lead coefficient, denominator, scalar solve --
+// all functions of the position): CMFW_TRAJ_OK, or the status of the first
+// failing step. A walk that passes can still fail on a non-finite or
+// all-zero matrix, which the walk itself checks.
+template <int P_, int Q_, int DIM>
+__device__ __forceinline__ int scan_failure(const WalkArgs &W, int t, int N) {
+    constexpr int NAX = (P_ > 0) ? (P_ + Q_) : CMFW_MAX_AXES;
+    constexpr int PM = (P_ > 0) ? P_ : 8;
+    constexpr int QM = (P_ > 0) ? Q_ : 7;
+    const int P = (P_ > 0) ? P_ : W.p;
+    const int Q = (P_ > 0) ? Q_ : W.q;
+    const int naxes = P + Q;
+    const cmfw_traj_in &in = W.in[t];
+    int absd[NAX];
+    uint32_t neg;
+    const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
+    if (maxabs < 0) return CMFW_TRAJ_STEP_CAP;
+    if (N <= 0 || W.h <= 0 || N - 2 * W.h <= 0) return CMFW_TRAJ_BAD_DEPTH;
+    double pos[NAX];
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) pos[a] = (a < naxes) ? in.start[a] : 0.0;
+    const StepConst K = make_step_const(P, Q, DIM, W.z);
+    for (int step = 1; step <= N; ++step) {
+        const int st = lattice_step_tests<DIM, NAX, PM, QM>(pos, absd, neg, maxabs, K);
+        if (st != CMFW_TRAJ_OK) return st;
+    }
+    return CMFW_TRAJ_OK;
+}
+
+}  // namespace cmfw

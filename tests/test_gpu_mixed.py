@@ -33,7 +33,9 @@ def test_mixed_equals_sequential_walks(cuda, variant):
     descs, recs, items = _batch(3000, 5)
     ref = _per_group(descs, recs, items, variant)
     assert (ref["valid"] == 1).sum() > 100
-    for tuning in (None, cmfw.baseline_tuning()):
+    scan = cmfw.MixedTuning()
+    scan.persistent, scan.prescan = 1, 1
+    for tuning in (None, cmfw.baseline_tuning(), scan):
         got = cmfw.walk_mixed(descs, recs, items, H, variant, tuning)
         assert got.tobytes() == ref.tobytes()
 
@@ -44,7 +46,7 @@ def test_mixed_graph_replay_and_autotune(cuda):
     b = cmfw.MixedBatch(descs, recs, items, H, "f64")
     t = b.autotune(sample=512)
     for f in range(len(descs)):
-        assert t.tile[f].block_size in (64, 128, 256) and t.tile[f].grab in (32, 64)
+        assert t.tile[f].block_size in (64, 128, 256) and t.tile[f].grab in (0, 32, 64)
     b.capture(t)
     for _ in range(2):  # replays reset the queues themselves
         b.d_out.fill_(0)
