@@ -99,3 +99,28 @@ def test_exact_estimator_matches_reference_formula():
     same = [Fraction(1, 4)] * 3
     assert exact.exact_estimator(same, 1) == Fraction(1, 4)
     assert exact.exact_estimator(None, 1) is None
+
+
+def test_proposal_helpers():
+    from cmfw import proposal as prop
+    t = prop.delta_target(np.array([0.0, 1.0, -1.0, 5397.0]))
+    assert t.dtype == np.float32
+    assert t[0] == 0.0 and abs(t[1] - np.log(2.0)) < 1e-6 and abs(t[2] + np.log(2.0)) < 1e-6
+    assert t[3] < 9.0 and prop.VALID_NAN < -1.0 and prop.FLOOR < prop.VALID_NAN
+    idx, d = prop.top_k(np.array([10, 11, 12, 13]), np.array([0.5, 3.0, -1.0, 3.0]), 2)
+    assert idx.tolist() == [11, 13] and d.tolist() == [3.0, 3.0]
+    assert prop.recall([1, 2, 3], [3, 4]) == 0.5
+    assert prop.recall([], []) == 1.0
+
+
+def test_mixed_batch_generator():
+    import cmfw.workloads as wl
+    d1, r1, i1 = wl.mixed_batch(500, 3)
+    d2, r2, i2 = wl.mixed_batch(500, 3)
+    assert r1.tobytes() == r2.tobytes() and i1.tobytes() == i2.tobytes()
+    assert len(d1) == 10 and i1["desc"].min() >= 0 and i1["desc"].max() <= 9
+    assert i1["N"].min() >= 200 and i1["N"].max() < 5000
+    for t in range(500):
+        p, q = wl.MIXED_FAMILIES[i1["desc"][t] // 2]
+        assert r1["dir"][t, :p + q].any() and not r1["dir"][t, p + q:].any()
+        assert ((r1["start"][t, :p + q] >= 1) & (r1["start"][t, :p + q] <= 10)).all()
