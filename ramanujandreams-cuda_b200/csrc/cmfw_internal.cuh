@@ -62,6 +62,38 @@ __device__ __forceinline__ uint32_t level_mask(const int (&absd)[NAX], int level
 
 __device__ __forceinline__ int top_axis(uint32_t mask) { return 31 - __clz(mask); }
 
+// One direction's axis-step order in run-length form, for kernels whose
+// threads all walk the same direction: the level masks change only at the
+// distinct values of |dir|, so levels thr[i] .. thr[i+1]+1 all step the axes
+// of mask[i] (thr[k] = 0). Held in shared memory, it keeps |dir| out of
+// every thread's registers.
+struct LevelPlan {
+    int k;
+    int thr[CMFW_MAX_AXES + 1];
+    uint32_t mask[CMFW_MAX_AXES];
+    uint32_t up;  // bit a set when axis a steps up (dir[a] >= 0)
+};
+
+template <int NAX>
+__device__ __forceinline__ void make_level_plan(const int (&absd)[NAX], uint32_t negmask, int maxabs,
+                                                LevelPlan &L) {
+    int k = 0, level = maxabs;
+    while (level >= 1) {
+        const uint32_t m = level_mask<NAX>(absd, level);
+        // the next distinct |dir| value below `level`
+        int next = 0;
+#pragma unroll
+        for (int a = 0; a < NAX; ++a) next = (absd[a] < level && absd[a] > next) ? absd[a] : next;
+        L.thr[k] = level;
+        L.mask[k] = m;
+        ++k;
+        level = next;
+    }
+    L.thr[k] = 0;
+    L.k = k;
+    L.up = ~negmask;
+}
+
 // ---------------------------------------------------------------------------
 // Snapshot reduction (cmf_pfq.cuh:385-596 and the result selection of
 // cmf_walk_f64.cu:122-153). `m` holds three dim x dim matrices (row stride

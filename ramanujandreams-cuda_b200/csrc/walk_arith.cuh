@@ -218,6 +218,36 @@ __device__ __forceinline__ bool healthy(const typename A::T (&m)[DIM][DIM]) {
     return any_nz && !bad;
 }
 
+// A trajectory position: a register array, or a thread's column of a
+// shared [NAX][NT] array (SmemPos), which frees 2 * NAX registers in
+// kernels whose walk state fills the register file.
+template <int NT>
+struct SmemPos {
+    double *p;  // &array[0][thread]
+    __device__ __forceinline__ double operator[](int a) const { return p[a * NT]; }
+};
+
+template <int NAX>
+__device__ __forceinline__ double pos_at(const double (&pos)[NAX], int axis) {
+    double v = 0.0;
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) v = (a == axis) ? pos[a] : v;
+    return v;
+}
+template <int NAX, int NT>
+__device__ __forceinline__ double pos_at(const SmemPos<NT> &pos, int axis) {
+    return pos[axis];
+}
+template <int NAX>
+__device__ __forceinline__ void pos_move(double (&pos)[NAX], int axis, double d) {
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) pos[a] += (a == axis) ? d : 0.0;
+}
+template <int NAX, int NT>
+__device__ __forceinline__ void pos_move(const SmemPos<NT> &pos, int axis, double d) {
+    pos.p[axis * NT] += d;
+}
+
 // Per-launch constants of the walk step.
 struct StepConst {
     int P, Q;
@@ -234,13 +264,13 @@ struct StepConst {
 // column of a forward step is skipped). Returns a cmfw_traj_status.
 template <int DIM>
 struct StepMatrix {
-    double col[DIM], be[DIM];
+    double col[DIM];
     double inva, sd;
     bool inverse;
 };
 
-template <bool FULL, int DIM, int NAX, int PM, int QM>
-__device__ __forceinline__ int step_matrix(const double (&pos)[NAX], int axis, bool up, const StepConst &K,
+template <bool FULL, int DIM, int NAX, int PM, int QM, class POS>
+__device__ __forceinline__ int step_matrix(const POS &pos, int axis, bool up, const StepConst &K,
                                            StepMatrix<DIM> &S) {
     const int P = K.P, Q = K.Q;
     const bool is_x = axis < P;
@@ -248,9 +278,7 @@ __device__ __forceinline__ int step_matrix(const double (&pos)[NAX], int axis, b
     S.inverse = inverse;
     // evaluation point: x- steps evaluate at x-1, y+ steps at y+1
     const double dlt = inverse ? (is_x ? -1.0 : 1.0) : 0.0;
-    double pa = 0.0;
-#pragma unroll
-    for (int a = 0; a < NAX; ++a) pa = (a == axis) ? pos[a] : pa;
+    const double pa = pos_at<NAX>(pos, axis);
     const double denom = up ? pa : pa - 1.0;
 
     double xv[PM], yv[QM > 0 ? QM : 1];
@@ -289,12 +317,13 @@ __device__ __forceinline__ int step_matrix(const double (&pos)[NAX], int axis, b
     if (inverse) {
         // back-substitution in t = out[DIM-1] (cmf_pfq.cuh:207-235); beta and
         // the scalar solve do not depend on the row
-        S.be[DIM - 1] = 1.0;
+        double be[DIM];
+        be[DIM - 1] = 1.0;
 #pragma unroll
-        for (int j = DIM - 2; j >= 0; --j) S.be[j] = -S.be[j + 1] * inva;
-        double db = S.be[0] * S.col[0];
+        for (int j = DIM - 2; j >= 0; --j) be[j] = -be[j + 1] * inva;
+        double db = be[0] * S.col[0];
 #pragma unroll
-        for (int k = 1; k < DIM; ++k) db = __fma_rn(S.be[k], S.col[k], db);
+        for (int k = 1; k < DIM; ++k) db = __fma_rn(be[k], S.col[k], db);
         const double sd = __fma_rn(db, inva, 1.0);
         const double ss = fmax(1.0, fabs(db * inva));
         if (!isfinite(sd) || fabs(sd) <= 128.0 * CMFW_EPS64 * ss) return CMFW_TRAJ_SINGULAR_SOLVE;
@@ -305,9 +334,9 @@ __device__ __forceinline__ int step_matrix(const double (&pos)[NAX], int axis, b
 
 // One axis step: M <- M (I + C/a) or M (I + C/a)^-1, then the position
 // moves by `up ? +1 : -1` along `axis`. Returns a cmfw_traj_status.
-template <int DIM, int NAX, int PM, int QM, class A>
-__device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], double (&pos)[NAX],
-                                         int axis, bool up, const StepConst &K) {
+template <int DIM, int NAX, int PM, int QM, class A, class POS>
+__device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], POS &pos, int axis, bool up,
+                                         const StepConst &K) {
     typedef typename A::T T;
     StepMatrix<DIM> S;
     const int st = step_matrix<true, DIM, NAX, PM, QM>(pos, axis, up, K, S);
@@ -338,14 +367,18 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)
 #pragma unroll
             for (int k = 1; k < DIM - 1; ++k) da = A::fma_s(al[k], S.col[k], da);
             const T tt = A::div_s(A::fma_s(da, ninva, m[r][DIM - 1]), S.sd, isd);
+            // beta_j = (-1/a)^(DIM-1-j), formed as in step_matrix
+            double bj = 1.0;
 #pragma unroll
-            for (int j = 0; j < DIM; ++j) m[r][j] = A::fma_s(tt, S.be[j], al[j]);
+            for (int j = DIM - 1; j >= 0; --j) {
+                m[r][j] = A::fma_s(tt, bj, al[j]);
+                bj = -bj * inva;
+            }
         }
     }
 #pragma unroll
     for (int r = 0; r < DIM; ++r) rescale<A, DIM>(m[r], ex[r]);
-#pragma unroll
-    for (int a = 0; a < NAX; ++a) pos[a] += (a == axis) ? (up ? 1.0 : -1.0) : 0.0;
+    pos_move<NAX>(pos, axis, up ? 1.0 : -1.0);
     return CMFW_TRAJ_OK;
 }
 
@@ -362,6 +395,27 @@ __device__ __forceinline__ int lattice_step(typename A::T (&m)[DIM][DIM], int (&
             mask &= ~(1u << axis);
             const int st = axis_step<DIM, NAX, PM, QM, A>(m, ex, pos, axis, !((neg >> axis) & 1u), K);
             if (st != CMFW_TRAJ_OK) return st;
+        }
+    }
+    return CMFW_TRAJ_OK;
+}
+
+// lattice_step with the direction read from a shared-memory LevelPlan.
+template <int DIM, int NAX, int PM, int QM, class A, class POS>
+__device__ __forceinline__ int lattice_step_plan(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], POS &pos,
+                                                 const LevelPlan &L, const StepConst &K) {
+    const int k = L.k;
+    for (int i = 0; i < k; ++i) {
+        const uint32_t lm = L.mask[i];
+        const int lo = L.thr[i + 1];
+        for (int level = L.thr[i]; level > lo; --level) {
+            uint32_t mask = lm;
+            while (mask) {
+                const int axis = top_axis(mask);
+                mask &= ~(1u << axis);
+                const int st = axis_step<DIM, NAX, PM, QM, A>(m, ex, pos, axis, (L.up >> axis) & 1u, K);
+                if (st != CMFW_TRAJ_OK) return st;
+            }
         }
     }
     return CMFW_TRAJ_OK;

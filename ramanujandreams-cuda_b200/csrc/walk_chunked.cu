@@ -104,10 +104,11 @@ __host__ __device__ constexpr int chunk_threads(int dim) { return dim <= 6 ? 256
 
 // CTA-cooperative products: every task multiplies two DIM x DIM matrices
 // (matrix-exponent form) in the combine arithmetic, one result entry per
-// work item spread over the NT threads; the entries are formed in registers
-// before any is stored (so a task may write over its first operand), and
-// each result is rescaled by a power of two so that its largest entry lies
-// in [1, 2) (per-task maximum through a shared atomic).
+// work item spread over the NT threads (ILP independent entries in flight
+// per thread); the entries go to a staging area first, so a task may write
+// over its first operand, and each result is rescaled by a power of two so
+// that its largest entry lies in [1, 2) (per-task maximum through a shared
+// atomic).
 template <class CA>
 struct ProdTask {
     const typename CA::T *a, *b;
@@ -116,37 +117,66 @@ struct ProdTask {
     int *ec;
 };
 
-template <int DIM, class CA, int NT, int MAXW>
-__device__ __forceinline__ void par_products(const ProdTask<CA> *tasks, int ntasks, int *pmax) {
+template <int DIM, class CA, int NT>
+__device__ __forceinline__ void par_products(const ProdTask<CA> *tasks, int ntasks, int *pmax,
+                                             typename CA::T *stage) {
     typedef typename CA::T CT;
     constexpr int DD = DIM * DIM;
-    CT acc[MAXW];
+    constexpr int ILP = 4;
+    const int nw = ntasks * DD;
+#pragma unroll 1
+    for (int w0 = threadIdx.x; w0 < nw; w0 += ILP * NT) {
+        CT x[ILP];
 #pragma unroll
-    for (int q = 0; q < MAXW; ++q) {
-        const int w = threadIdx.x + q * NT;
-        if (w < ntasks * DD) {
-            const ProdTask<CA> &T = tasks[w / DD];
-            const int e = w % DD, i = e / DIM, j = e % DIM;
-            CT x = CA::mul(T.a[i * DIM], T.b[j]);
+        for (int u = 0; u < ILP; ++u) {
+            const int w = w0 + u * NT;
+            if (w < nw) {
+                const ProdTask<CA> &T = tasks[w / DD];
+                const int e = w % DD, i = e / DIM, j = e % DIM;
+                x[u] = CA::mul(T.a[i * DIM], T.b[j]);
 #pragma unroll
-            for (int k = 1; k < DIM; ++k) x = CA::fma(T.a[i * DIM + k], T.b[k * DIM + j], x);
-            acc[q] = x;
-            atomicMax(&pmax[w / DD], CA::hexp(x));
+                for (int k = 1; k < DIM; ++k) x[u] = CA::fma(T.a[i * DIM + k], T.b[k * DIM + j], x[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < ILP; ++u) {
+            const int w = w0 + u * NT;
+            if (w < nw) {
+                stage[w] = x[u];
+                atomicMax(&pmax[w / DD], CA::hexp(x[u]));
+            }
         }
     }
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < MAXW; ++q) {
-        const int w = threadIdx.x + q * NT;
-        if (w < ntasks * DD) {
-            const ProdTask<CA> &T = tasks[w / DD];
-            const int hm = pmax[w / DD];
-            const int be = (hm != 0 && hm < 0x7ff00000) ? (hm >> 20) - 1023 : 0;
-            T.c[w % DD] = CA::scale(acc[q], be);
-            if (w % DD == 0) *T.ec = T.ea + T.eb + be;
-        }
+#pragma unroll 1
+    for (int w = threadIdx.x; w < nw; w += NT) {
+        const ProdTask<CA> &T = tasks[w / DD];
+        const int hm = pmax[w / DD];
+        const int be = (hm != 0 && hm < 0x7ff00000) ? (hm >> 20) - 1023 : 0;
+        T.c[w % DD] = CA::scale(stage[w], be);
+        if (w % DD == 0) *T.ec = T.ea + T.eb + be;
     }
     __syncthreads();
+}
+
+// Dynamic shared memory of the chunk kernel: NT run products + 6 work
+// matrices, their exponents, NT/2 product tasks with their maxima, and one
+// region that holds the threads' positions during the runs and the
+// products' staging area afterwards.
+template <class CT>
+__host__ __device__ constexpr size_t chunk_union_bytes(int dim, int nt) {
+    return (size_t)CMFW_MAX_AXES * nt * sizeof(double) > (size_t)(nt / 2) * dim * dim * sizeof(CT)
+               ? (size_t)CMFW_MAX_AXES * nt * sizeof(double)
+               : (size_t)(nt / 2) * dim * dim * sizeof(CT);
+}
+template <class CT>
+__host__ __device__ constexpr size_t chunk_union_offset(int dim, int nt) {
+    return ((size_t)(nt + 6) * dim * dim * sizeof(CT) + (nt + 6) * sizeof(int) + 15) / 16 * 16 +
+           (size_t)(nt / 2) * (sizeof(ProdTask<ArithF64>) + sizeof(int));
+}
+template <class CT>
+__host__ __device__ constexpr size_t chunk_smem_bytes(int dim, int nt) {
+    return (chunk_union_offset<CT>(dim, nt) + 15) / 16 * 16 + chunk_union_bytes<CT>(dim, nt);
 }
 
 // CTAs per cluster of the chunk kernel: a trajectory is walked by one CTA,
@@ -166,16 +196,19 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
     constexpr int PM = (P_ > 0) ? P_ : 8;
     constexpr int QM = (P_ > 0) ? Q_ : 7;
     constexpr int DD = DIM * DIM;
-    constexpr int MAXW = (DD + 1) / 2;          // work items per thread in a tree level
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT *smem = (CT *)smem_raw;                  // NT run products + 6 work matrices
     int *sexp = (int *)(smem + (NT + 6) * DD);  // NT + 6 exponents
     ProdTask<CA> *tasks = (ProdTask<CA> *)(((uintptr_t)(sexp + NT + 6) + 15) & ~(uintptr_t)15);  // NT / 2
     int *pmax = (int *)(tasks + NT / 2);        // NT / 2
+    unsigned char *ureg = smem_raw + (chunk_union_offset<CT>(DIM, NT) + 15) / 16 * 16;
+    double *s_pos = (double *)ureg;             // during the runs: [NAX][NT] positions
+    CT *stage = (CT *)ureg;                     // afterwards: product staging
     __shared__ int s_ntask, s_fkey, s_ok;
     __shared__ double s_ls[3];
     // earliest failing lattice step of this CTA's runs, as step * 16 + status
     __shared__ int s_fail;
+    __shared__ LevelPlan s_plan;
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
     const int tid = threadIdx.x;
@@ -193,32 +226,25 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
     const int NTOT = NT * NP;
 
     // segments of lattice steps and the runs (global index g over the NP
-    // CTAs) that cover them; the same for every trajectory of the launch
-    const int S = 0;
-    const int cp1 = W.N - 2 * W.h, cp2 = W.N - W.h;
-    const int L0 = cp1 - S, L1 = W.h, L2 = W.h;
-    const int rest = W.N - S;
-    int T1 = (NTOT * L1 + rest / 2) / rest;
-    T1 = max(1, min(T1, L1));
-    int T2 = max(1, min(T1, L2));
-    const int T0 = NTOT - T1 - T2;
-    const int segbase[3] = {0, T0, T0 + T1}, segT[3] = {T0, T1, T2};
-    const int g = part * NT + tid;
-    const int seg = g < T0 ? 0 : (g < T0 + T1 ? 1 : 2);
-    const int Lseg = seg == 0 ? L0 : (seg == 1 ? L1 : L2);
-    const int first = seg == 0 ? S + 1 : (seg == 1 ? cp1 + 1 : cp2 + 1);
-    const int local = g - segbase[seg];
-    const int lo = first + (int)(((long long)local * Lseg) / segT[seg]);
-    const int hi = first + (int)(((long long)(local + 1) * Lseg) / segT[seg]);
-    // this CTA's share [cbeg, cend) of each segment's runs, in CTA thread ids
-    int cbeg[3], ccnt[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int b0 = max(segbase[k], part * NT), b1 = min(segbase[k] + segT[k], (part + 1) * NT);
-        cbeg[k] = b0 - part * NT;
-        ccnt[k] = max(0, b1 - b0);
+    // CTAs) that cover them; the same for every trajectory of the launch.
+    // Kept in shared memory and re-derived where needed, so that none of it
+    // holds a register across the runs.
+    __shared__ int s_segbase[3], s_segT[3];
+    if (tid == 0) {
+        const int rest = W.N;
+        int T1 = (NTOT * W.h + rest / 2) / rest;
+        T1 = max(1, min(T1, W.h));
+        const int T2 = max(1, min(T1, W.h));
+        const int T0 = NTOT - T1 - T2;
+        s_segbase[0] = 0;
+        s_segbase[1] = T0;
+        s_segbase[2] = T0 + T1;
+        s_segT[0] = T0;
+        s_segT[1] = T1;
+        s_segT[2] = T2;
     }
-    const int lrel = tid - cbeg[seg];  // index among this CTA's runs of the segment
+    __syncthreads();
+    const int g = part * NT + tid;
 
     for (int round = 0;; ++round) {
         const int b0 = (round * nclusters + (int)(blockIdx.x / CL)) * per_cluster;
@@ -226,7 +252,15 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
         const int b = b0 + sub;
         const bool active = b < count;
         const int t = active ? C.list[b] : 0;
-        if (tid == 0) s_fail = 0x7fffffff;
+        if (tid == 0) {
+            s_fail = 0x7fffffff;
+            if (active) {
+                int absd[NAX];
+                uint32_t neg;
+                const int maxabs = load_direction<NAX>(W.in[t], naxes, absd, neg);
+                make_level_plan<NAX>(absd, neg, maxabs, s_plan);
+            }
+        }
         T m[DIM][DIM];
         int ex[DIM];
 #pragma unroll
@@ -237,20 +271,24 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
         }
         __syncthreads();
         if (active) {
+            // this thread's run [lo, hi) of lattice steps
+            const int seg = g < s_segbase[1] ? 0 : (g < s_segbase[2] ? 1 : 2);
+            const int Lseg = seg == 0 ? W.N - 2 * W.h : W.h;
+            const int first = seg == 0 ? 1 : (seg == 1 ? W.N - 2 * W.h + 1 : W.N - W.h + 1);
+            const int local = g - s_segbase[seg];
+            const int lo = first + (int)(((long long)local * Lseg) / s_segT[seg]);
+            const int hi = first + (int)(((long long)(local + 1) * Lseg) / s_segT[seg]);
             const cmfw_traj_in &in = W.in[t];
-            int absd[NAX];
-            uint32_t neg;
-            const int maxabs = load_direction<NAX>(in, naxes, absd, neg);
-            double pos[NAX];
+            const SmemPos<NT> pos{s_pos + tid};
 #pragma unroll
             for (int a = 0; a < NAX; ++a) {
                 const double d = (a < naxes) ? (double)in.dir[a] : 0.0;
-                pos[a] = (a < naxes) ? in.start[a] + (double)(lo - 1) * d : 0.0;
+                pos.p[a * NT] = (a < naxes) ? in.start[a] + (double)(lo - 1) * d : 0.0;
             }
             volatile int *fail = &s_fail;
             for (int step = lo; step < hi; ++step) {
                 if (*fail < step * 16) break;  // an earlier step failed: this run is moot
-                int st = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
+                int st = lattice_step_plan<DIM, NAX, PM, QM, A>(m, ex, pos, s_plan, K);
                 if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
                 if (st != CMFW_TRAJ_OK) {
                     atomicMin(&s_fail, step * 16 + st);
@@ -260,12 +298,22 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
         }
         sexp[tid] = to_matrix_exponent<DIM, A>(m, ex, smem + tid * DD);
         __syncthreads();
+        // this CTA's share of its segment's runs: lrel = index among them,
+        // ccnt = their number
+        int lrel, ccnt;
+        {
+            const int seg = g < s_segbase[1] ? 0 : (g < s_segbase[2] ? 1 : 2);
+            const int b0 = max(s_segbase[seg], part * NT);
+            const int b1 = min(s_segbase[seg] + s_segT[seg], (part + 1) * NT);
+            lrel = tid - (b0 - part * NT);
+            ccnt = max(0, b1 - b0);
+        }
         // in-order tree product of this CTA's runs of each segment, one
         // level at a time, every level's products spread over the CTA
         for (int stride = 1; stride < NT; stride <<= 1) {
             if (tid == 0) s_ntask = 0;
             __syncthreads();
-            if (active && (lrel % (2 * stride)) == 0 && lrel + stride < ccnt[seg]) {
+            if (active && (lrel % (2 * stride)) == 0 && lrel + stride < ccnt) {
                 const int q = atomicAdd(&s_ntask, 1);
                 tasks[q] = ProdTask<CA>{smem + tid * DD, smem + (tid + stride) * DD, smem + tid * DD, sexp[tid],
                                         sexp[tid + stride], &sexp[tid]};
@@ -274,7 +322,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
             __syncthreads();
             const int nt = s_ntask;
             if (nt == 0) break;  // no segment has runs this far apart
-            par_products<DIM, CA, NT, MAXW>(tasks, nt, pmax);
+            par_products<DIM, CA, NT>(tasks, nt, pmax, stage);
         }
         // every part's products and failure key are final (CTAs that walk
         // alone need no cluster barrier)
@@ -301,7 +349,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
                     const CT *pm[2];
                     int pe[2], np = 0;
                     for (int q = 0; q < NP; ++q) {
-                        const int b0q = max(segbase[k], q * NT), b1q = min(segbase[k] + segT[k], (q + 1) * NT);
+                        const int b0q = max(s_segbase[k], q * NT), b1q = min(s_segbase[k] + s_segT[k], (q + 1) * NT);
                         if (b1q <= b0q) continue;
                         const int slot = b0q - q * NT;
                         pm[np] = cluster.map_shared_rank(smem, crank + q) + slot * DD;
@@ -318,7 +366,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
                     }
                 }
                 __syncthreads();
-                if (s_ntask > 0) par_products<DIM, CA, NT, MAXW>(tasks, s_ntask, pmax);
+                if (s_ntask > 0) par_products<DIM, CA, NT>(tasks, s_ntask, pmax, stage);
                 // snapshots: seg0, then * seg1, then * seg2
                 for (int i = tid; i < DD; i += NT) x[i] = y[i];
                 if (tid == 0) xe[0] = ye[0];
@@ -329,7 +377,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
                         pmax[0] = 0;
                     }
                     __syncthreads();
-                    par_products<DIM, CA, NT, MAXW>(tasks, 1, pmax);
+                    par_products<DIM, CA, NT>(tasks, 1, pmax, stage);
                 }
                 double *snap = W.snap + (size_t)t * 3 * DD;
                 int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
@@ -431,8 +479,7 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     C.count = (int *)p;
     C.prefix_steps = prefix_steps;
     const int NT = chunk_threads(dim);
-    const size_t shmem = (size_t)(NT + 6) * dim * dim * sizeof(typename A::Combine::T) + (NT + 6) * sizeof(int) + 16 +
-                         (size_t)(NT / 2) * (sizeof(ProdTask<typename A::Combine>) + sizeof(int));
+    const size_t shmem = chunk_smem_bytes<typename A::Combine::T>(dim, NT);
     cudaError_t e = cudaFuncSetAttribute((const void *)k.chunk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shmem);
     if (e != cudaSuccess) return e;
