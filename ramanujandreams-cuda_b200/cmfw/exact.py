@@ -178,11 +178,32 @@ def exact_estimator(rs, method):
     return r3
 
 
+def rounding_floor(rs, method, u=Fraction(1, 2 ** 51)):
+    """The estimator's relative change when each exact ratio moves by a
+    relative u (4 units of 2^-53 by default): the error that computing the
+    ratios in double precision alone can leave in the limit, however exact
+    the walk. Aitken's estimator divides by a second difference of the
+    ratios, so on partially converged walks this floor reaches 1e-10 and
+    beyond. None where the estimator has no exact value."""
+    L = exact_estimator(rs, method)
+    if L is None or L == 0:
+        return None
+    worst = Fraction(0)
+    for signs in ((a, b, c) for a in (-1, 1) for b in (-1, 1) for c in (-1, 1)):
+        moved = [r * (1 + sg * u) for r, sg in zip(rs, signs)]
+        Lm = exact_estimator(moved, method)
+        if Lm is None:
+            return math.inf
+        worst = max(worst, abs(Lm - L) / abs(L))
+    return float(worst)
+
+
 def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=1024):
     """Per-trajectory exact check of float results.
 
     Returns a dict of arrays: verified (bool), rel_err (float, nan where not
-    comparable), exact_limit (float), K (primes used).
+    comparable), exact_limit (float), K (primes used), floor (float: the
+    rounding_floor of the trajectory's estimator, nan where undefined).
     """
     n = len(records)
     valid = np.asarray(results["valid"]) == 1
@@ -192,6 +213,7 @@ def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=1024):
     rel = np.full(n, np.nan)
     exact_limit = np.full(n, np.nan)
     Ks = np.zeros(n, dtype=np.int64)
+    floor = np.full(n, np.nan)
     if len(idx):
         ratios, K_used = exact_ratios(desc, records[idx], N, h, pairs=src[idx] & 0xFFF, K0=K0)
         for li, t in enumerate(idx):
@@ -199,6 +221,8 @@ def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=1024):
             L = exact_estimator(ratios[li], (int(src[t]) >> 12) & 1)
             if L is None:
                 continue
+            fl = rounding_floor(ratios[li], (int(src[t]) >> 12) & 1)
+            floor[t] = np.nan if fl is None else fl
             try:
                 exact_limit[t] = float(L)
             except OverflowError:  # beyond the double range: no double is within rtol
@@ -212,7 +236,7 @@ def verify(desc, records, results, limit_src, N, h, rtol=1e-10, K0=1024):
                 err = abs(Fraction(lf) - L) / abs(L)
             rel[t] = float(err) if err < 1e300 else math.inf
             verified[t] = rel[t] <= rtol
-    return {"verified": verified, "rel_err": rel, "exact_limit": exact_limit, "K": Ks}
+    return {"verified": verified, "rel_err": rel, "exact_limit": exact_limit, "K": Ks, "floor": floor}
 
 
 def export_topk(desc, records, results, N, h, k=100, K0=1024):

@@ -193,10 +193,11 @@ class DeltaSearch:
         net.status()
         return ti, td, int(sel.numel()), n_valid, {"score": c_score.ms, "select": c_select.ms, "walk": c_walk.ms}
 
-    def confirm(self, indices, limits=None, rtol=1e-10):
+    def confirm(self, indices, limits=None, rtol=1e-10, detail=False):
         """Exact check of the reported trajectories' f64 limits (the walk
         repeated in f64 with its limit source, against the exact rational
-        walk); returns the number verified."""
+        walk); returns the number verified, or with detail=True the
+        exact.verify record (errors and rounding floors per trajectory)."""
         torch = api._torch()
         if len(indices) == 0:
             return 0
@@ -205,7 +206,7 @@ class DeltaSearch:
         recs = recs_dev.cpu().numpy().reshape(-1).view(api.IN_DTYPE).copy()
         out, src = api.walk("f64", self.desc, recs, self.N, self.h, with_limit_src=True)
         v = exact.verify(self.desc, recs, out, src, self.N, self.h, rtol=rtol)
-        return int(v["verified"].sum())
+        return v if detail else int(v["verified"].sum())
 
 
 def recall(found, truth):

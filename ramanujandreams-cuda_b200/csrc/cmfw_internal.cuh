@@ -72,6 +72,7 @@ struct LevelPlan {
     int thr[CMFW_MAX_AXES + 1];
     uint32_t mask[CMFW_MAX_AXES];
     uint32_t up;  // bit a set when axis a steps up (dir[a] >= 0)
+    int L;        // axis steps per lattice step, sum of |dir|
 };
 
 template <int NAX>
@@ -92,6 +93,9 @@ __device__ __forceinline__ void make_level_plan(const int (&absd)[NAX], uint32_t
     L.thr[k] = 0;
     L.k = k;
     L.up = ~negmask;
+    int n = 0;
+    for (int i = 0; i < k; ++i) n += (L.thr[i] - L.thr[i + 1]) * __popc(L.mask[i]);
+    L.L = n;
 }
 
 // ---------------------------------------------------------------------------

@@ -205,6 +205,21 @@ __device__ __forceinline__ void rescale(typename A::T (&row)[DIM], int &e) {
     }
 }
 
+// healthy() over the R rows a thread holds: bit 0 = some entry non-zero,
+// bit 1 = some entry non-finite (threads that share a walk combine them).
+template <class A, int R, int DIM>
+__device__ __forceinline__ int health_bits(const typename A::T (&m)[R][DIM]) {
+    bool any_nz = false, bad = false;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) {
+            bad |= A::hexp(m[r][j]) == 0x7ff00000;
+            any_nz |= A::nonzero(m[r][j]);
+        }
+    return (any_nz ? 1 : 0) | (bad ? 2 : 0);
+}
+
 template <class A, int DIM>
 __device__ __forceinline__ bool healthy(const typename A::T (&m)[DIM][DIM]) {
     bool any_nz = false, bad = false;
@@ -334,8 +349,10 @@ __device__ __forceinline__ int step_matrix(const POS &pos, int axis, bool up, co
 
 // One axis step: M <- M (I + C/a) or M (I + C/a)^-1, then the position
 // moves by `up ? +1 : -1` along `axis`. Returns a cmfw_traj_status.
-template <int DIM, int NAX, int PM, int QM, class A, class POS>
-__device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], POS &pos, int axis, bool up,
+// The rows of the walk matrix evolve independently (row r of M A is row r
+// of M times A), so a thread may hold any R of them: m[R][DIM].
+template <int DIM, int NAX, int PM, int QM, class A, int R, class POS>
+__device__ __forceinline__ int axis_step(typename A::T (&m)[R][DIM], int (&ex)[R], POS &pos, int axis, bool up,
                                          const StepConst &K) {
     typedef typename A::T T;
     StepMatrix<DIM> S;
@@ -345,7 +362,7 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)
     if (!S.inverse) {
         // out[j] = m[j] + m[j+1]/a, last += (m . col)/a
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) {
+        for (int r = 0; r < R; ++r) {
             T dot = A::mul_s(m[r][0], S.col[0]);
 #pragma unroll
             for (int k = 1; k < DIM; ++k) dot = A::fma_s(m[r][k], S.col[k], dot);
@@ -357,7 +374,7 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)
         const double isd = 1.0 / S.sd;
         const double ninva = -inva;
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) {
+        for (int r = 0; r < R; ++r) {
             T al[DIM];
             al[DIM - 1] = A::from(0.0);
             al[DIM - 2] = m[r][DIM - 2];
@@ -377,7 +394,7 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[DIM][DIM], int (&ex)
         }
     }
 #pragma unroll
-    for (int r = 0; r < DIM; ++r) rescale<A, DIM>(m[r], ex[r]);
+    for (int r = 0; r < R; ++r) rescale<A, DIM>(m[r], ex[r]);
     pos_move<NAX>(pos, axis, up ? 1.0 : -1.0);
     return CMFW_TRAJ_OK;
 }
@@ -395,27 +412,6 @@ __device__ __forceinline__ int lattice_step(typename A::T (&m)[DIM][DIM], int (&
             mask &= ~(1u << axis);
             const int st = axis_step<DIM, NAX, PM, QM, A>(m, ex, pos, axis, !((neg >> axis) & 1u), K);
             if (st != CMFW_TRAJ_OK) return st;
-        }
-    }
-    return CMFW_TRAJ_OK;
-}
-
-// lattice_step with the direction read from a shared-memory LevelPlan.
-template <int DIM, int NAX, int PM, int QM, class A, class POS>
-__device__ __forceinline__ int lattice_step_plan(typename A::T (&m)[DIM][DIM], int (&ex)[DIM], POS &pos,
-                                                 const LevelPlan &L, const StepConst &K) {
-    const int k = L.k;
-    for (int i = 0; i < k; ++i) {
-        const uint32_t lm = L.mask[i];
-        const int lo = L.thr[i + 1];
-        for (int level = L.thr[i]; level > lo; --level) {
-            uint32_t mask = lm;
-            while (mask) {
-                const int axis = top_axis(mask);
-                mask &= ~(1u << axis);
-                const int st = axis_step<DIM, NAX, PM, QM, A>(m, ex, pos, axis, (L.up >> axis) & 1u, K);
-                if (st != CMFW_TRAJ_OK) return st;
-            }
         }
     }
     return CMFW_TRAJ_OK;

@@ -5,30 +5,35 @@
 // into chunks walked independently and multiplied back together in order.
 // Two kernels:
 //
-//  1. filter: one thread per trajectory walks the first S lattice steps in
-//     plain FP64 (S = min(prefix_steps, N-2h-1)) and keeps nothing but the
-//     verdict: a trajectory that fails there is written invalid with its
-//     status, a survivor appends its index to a list. Most trajectories
-//     that fail, fail here (zeta starts hit a singular lead coefficient on
-//     their first y+ step). The step's singularity tests use the FP64
-//     column, denominators and solve, which every arithmetic forms the same
-//     way, so the verdict is the run arithmetic's.
-//  2. chunk: clusters of 2 CTAs of NT threads (256 up to rank 6, else 128)
-//     on a persistent grid that strides over the survivor list; each
-//     survivor is walked by one CTA, or by both CTAs of a cluster when there
-//     are fewer survivors than half the CTAs (the parts are multiplied in
-//     order through distributed shared memory). Steps 1..N form three
-//     segments [1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the snapshot depths are
-//     segment ends); each thread walks a contiguous run of lattice steps of
-//     one segment with the same registers-only step as the sequential
-//     kernel, the runs of a segment are multiplied in order by a
-//     shared-memory tree, and the leader CTA forms the three snapshots
-//     seg0, seg0 * seg1, seg0 * seg1 * seg2 and reduces them.
+//  1. filter: one thread per trajectory runs the singularity tests of the
+//     first S lattice steps (S = min(prefix_steps, N-2h-1)) without any
+//     matrix work and keeps nothing but the verdict: a trajectory that
+//     fails there is written invalid with its status, a survivor appends
+//     its index to a list. Most trajectories that fail, fail here (zeta
+//     starts hit a singular lead coefficient on their first y+ step). The
+//     tests depend on the position only (FP64 column, denominators and
+//     solve, which every arithmetic forms the same way), so the verdict is
+//     the run arithmetic's; the survivors' first steps are walked again by
+//     the chunk kernel's runs.
+//  2. chunk: CTAs of NT threads (256 up to rank 6, else 128) on a
+//     persistent grid; each survivor is walked by NP CTAs ("parts"), NP as
+//     large as the survivors leave CTAs for (at most kMaxParts). Steps
+//     1..N form three segments [1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the
+//     snapshot depths are segment ends). Every segment's axis steps are
+//     split evenly over its runs, one run per thread, so a run may start
+//     and end inside a lattice step; each thread walks its run with the
+//     same registers-only step as the sequential kernel, and a CTA
+//     multiplies its runs of each segment in order by a shared-memory
+//     tree. A trajectory walked in parts is finished by the part that
+//     ends last: the parts publish their segment products to global
+//     memory and count themselves in, and the last one to arrive (no CTA
+//     ever waits for another) multiplies them in order, forms the three
+//     snapshots seg0, seg0 * seg1, seg0 * seg1 * seg2 and reduces them.
 //
 // The latency of one trajectory drops from N lattice steps to about
-// N / (NP * NT) lattice steps + log2 NT matrix products; the total
-// arithmetic is that of the sequential walk plus NP * NT - 1 dense rank^3
-// products.
+// N * L / (NP * NT) axis steps (L = sum |dir|) + log2 NT + log2 NP matrix
+// products; the total arithmetic is that of the sequential walk plus
+// NP * NT - 1 dense rank^3 products.
 //
 // Accuracy. Multiplying runs together is a different association of the
 // same matrix product. A run started from the identity can pass through
@@ -43,25 +48,30 @@
 // in the sequential walk. CMFW_F_PLAIN_RUNS selects plain-FP64 runs (fewer
 // instructions, no such guarantee); df64 runs in float-float with FP64
 // products (ArithFF).
-#include <cooperative_groups.h>
+#include <algorithm>
 
 #include "walk_arith.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace cmfw {
 
 struct ChunkArgs {
     WalkArgs w;
-    int *list;     // n_traj survivor indices
-    int *count;    // survivors
+    int *list;                        // n_traj survivor indices
+    int *count;                       // survivors
+    int *arrive;                      // nslots: parts finished, per survivor walked in parts
+    void *parts;                      // nslots x 3 segment products of the parts (combine arithmetic)
+    int *parts_e;                     // nslots x 3 their exponents
+    unsigned long long *parts_fail;   // nslots earliest failure keys
+    int nslots;
     int prefix_steps;
 };
 
+// Threads per CTA of the filter kernel: 64, so that a batch of 10^4
+// trajectories spreads over every SM.
+constexpr int kFilterThreads = 64;
+
 template <int P_, int Q_, int DIM>
-__global__ void __launch_bounds__(128) walk_prefix_kernel(ChunkArgs C) {
-    typedef ArithF64 A;
-    typedef typename A::T T;
+__global__ void __launch_bounds__(kFilterThreads) walk_prefix_kernel(ChunkArgs C) {
     const WalkArgs &W = C.w;
     constexpr int NAX = (P_ > 0) ? (P_ + Q_) : CMFW_MAX_AXES;
     constexpr int PM = (P_ > 0) ? P_ : 8;
@@ -80,27 +90,27 @@ __global__ void __launch_bounds__(128) walk_prefix_kernel(ChunkArgs C) {
     double pos[NAX];
 #pragma unroll
     for (int a = 0; a < NAX; ++a) pos[a] = (a < naxes) ? in.start[a] : 0.0;
-    T m[DIM][DIM];
-    int ex[DIM];
-#pragma unroll
-    for (int r = 0; r < DIM; ++r) {
-        ex[r] = 0;
-#pragma unroll
-        for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r == j) ? 1.0 : 0.0);
-    }
     const StepConst K = make_step_const(P, Q, DIM, W.z);
+    // The singularity tests alone: a step that would leave the walk matrix
+    // non-finite without failing a test is found by the chunk kernel at the
+    // same lattice step (its runs test the matrix at every lattice-step end)
     const int S = min(C.prefix_steps, W.N - 2 * W.h - 1);
     for (int step = 1; step <= S; ++step) {
-        int st = lattice_step<DIM, NAX, PM, QM, A>(m, ex, pos, absd, neg, maxabs, K);
-        if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
+        const int st = lattice_step_tests<DIM, NAX, PM, QM>(pos, absd, neg, maxabs, K);
         if (st != CMFW_TRAJ_OK) { write_invalid(W, t, st); return; }
     }
     C.list[atomicAdd(C.count, 1)] = t;
 }
 
-// Threads per trajectory: 256 while a thread's registers allow (ranks up to
-// 6), 128 above.
-__host__ __device__ constexpr int chunk_threads(int dim) { return dim <= 6 ? 256 : 128; }
+// Threads per CTA of the chunk kernel, and threads per run: up to rank 6 a
+// thread holds a run's whole walk state (25 or 36 double-double entries);
+// from rank 7 two adjacent threads share a run, each with half the rows
+// (the rows of a walk evolve independently), since 49 or 64 double-double
+// entries would not fit one thread's registers. Runs, and shared product
+// slots, per CTA = threads / threads per run.
+__host__ __device__ constexpr int chunk_threads(int dim) { return 256; }
+__host__ __device__ constexpr int chunk_pair(int dim) { return dim >= 7 ? 2 : 1; }
+__host__ __device__ constexpr int chunk_runs(int dim) { return chunk_threads(dim) / chunk_pair(dim); }
 
 // CTA-cooperative products: every task multiplies two DIM x DIM matrices
 // (matrix-exponent form) in the combine arithmetic, one result entry per
@@ -159,35 +169,181 @@ __device__ __forceinline__ void par_products(const ProdTask<CA> *tasks, int ntas
     __syncthreads();
 }
 
-// Dynamic shared memory of the chunk kernel: NT run products + 6 work
-// matrices, their exponents, NT/2 product tasks with their maxima, and one
-// region that holds the threads' positions during the runs and the
-// products' staging area afterwards.
+// Dynamic shared memory of the chunk kernel: RT run products + 3 snapshot
+// matrices (RT = runs per CTA), their exponents, RT/2 product tasks with
+// their maxima, and one region that holds the threads' positions during
+// the runs and the products' staging area afterwards. (Static: the
+// threads' run ends and the per-launch geometry, about 2.4 KB; rank 6 in
+// double-double, the largest user, stays below the 227 KB a CTA may hold.)
 template <class CT>
-__host__ __device__ constexpr size_t chunk_union_bytes(int dim, int nt) {
-    return (size_t)CMFW_MAX_AXES * nt * sizeof(double) > (size_t)(nt / 2) * dim * dim * sizeof(CT)
-               ? (size_t)CMFW_MAX_AXES * nt * sizeof(double)
-               : (size_t)(nt / 2) * dim * dim * sizeof(CT);
+__host__ __device__ constexpr size_t chunk_union_bytes(int dim) {
+    return (size_t)CMFW_MAX_AXES * chunk_threads(dim) * sizeof(double) >
+                   (size_t)(chunk_runs(dim) / 2) * dim * dim * sizeof(CT)
+               ? (size_t)CMFW_MAX_AXES * chunk_threads(dim) * sizeof(double)
+               : (size_t)(chunk_runs(dim) / 2) * dim * dim * sizeof(CT);
 }
 template <class CT>
-__host__ __device__ constexpr size_t chunk_union_offset(int dim, int nt) {
-    return ((size_t)(nt + 6) * dim * dim * sizeof(CT) + (nt + 6) * sizeof(int) + 15) / 16 * 16 +
-           (size_t)(nt / 2) * (sizeof(ProdTask<ArithF64>) + sizeof(int));
+__host__ __device__ constexpr size_t chunk_union_offset(int dim) {
+    return ((size_t)(chunk_runs(dim) + 3) * dim * dim * sizeof(CT) + (chunk_runs(dim) + 3) * sizeof(int) + 15) /
+               16 * 16 +
+           (size_t)(chunk_runs(dim) / 2) * (sizeof(ProdTask<ArithF64>) + sizeof(int));
 }
 template <class CT>
-__host__ __device__ constexpr size_t chunk_smem_bytes(int dim, int nt) {
-    return (chunk_union_offset<CT>(dim, nt) + 15) / 16 * 16 + chunk_union_bytes<CT>(dim, nt);
+__host__ __device__ constexpr size_t chunk_smem_bytes(int dim) {
+    return (chunk_union_offset<CT>(dim) + 15) / 16 * 16 + chunk_union_bytes<CT>(dim);
 }
 
-// CTAs per cluster of the chunk kernel: a trajectory is walked by one CTA,
-// or by both CTAs of a cluster when the survivors leave enough SMs (chosen
-// on the device from the number of survivors).
-constexpr int kChunkCluster = 2;
+// In-order products of up to three groups of consecutive shared-memory
+// matrices (matrix-exponent form): group k holds slots gbase[k] ..
+// gbase[k] + gcnt[k] - 1 and ends with its product in slot gbase[k]. Thread
+// i looks after slot i; every tree level's products are spread over the CTA.
+template <int DIM, class CA, int NT>
+__device__ __forceinline__ void group_products(typename CA::T *slots, int *sexp, const int *gbase, const int *gcnt,
+                                               ProdTask<CA> *tasks, int *pmax, typename CA::T *stage, int *ntask) {
+    constexpr int DD = DIM * DIM;
+    const int tid = threadIdx.x;
+    int rel = -1, cnt = 0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        if (tid >= gbase[q] && tid < gbase[q] + gcnt[q]) {
+            rel = tid - gbase[q];
+            cnt = gcnt[q];
+        }
+    for (int stride = 1; stride < NT; stride <<= 1) {
+        if (tid == 0) *ntask = 0;
+        __syncthreads();
+        if (rel >= 0 && (rel % (2 * stride)) == 0 && rel + stride < cnt) {
+            const int q = atomicAdd(ntask, 1);
+            tasks[q] = ProdTask<CA>{slots + tid * DD, slots + (tid + stride) * DD, slots + tid * DD, sexp[tid],
+                                    sexp[tid + stride], &sexp[tid]};
+            pmax[q] = 0;
+        }
+        __syncthreads();
+        const int nt = *ntask;
+        if (nt == 0) break;  // no group has members this far apart
+        par_products<DIM, CA, NT>(tasks, nt, pmax, stage);
+    }
+}
+
+// Failure key of axis step a (0-based over the whole walk): the earliest
+// failing step of a trajectory is the smallest key.
+__device__ __forceinline__ unsigned long long fail_key(long long a, int status) {
+    return ((unsigned long long)a << 4) | (unsigned)status;
+}
+constexpr unsigned long long kNoFailure = ~0ull;
+
+// Lanes of the thread pair that shares a run (G = 2), for shuffles.
+__device__ __forceinline__ unsigned pair_mask() { return 3u << ((threadIdx.x & 31) & ~1u); }
+
+// Walks axis steps [alo, *ahi) of a trajectory into the R rows m that this
+// thread holds (G threads share a run, each with its own rows and the same
+// position sequence). Axis step a is step a % L (in the plan's order) of
+// lattice step a / L + 1, L the plan's axis steps per lattice step; pos
+// holds the position at the start of lattice step alo / L + 1. Failures go
+// to *fail as fail_key; at each lattice-step end the walk stops early if a
+// smaller key is there. The non-finite test of the sequential walk runs at
+// every lattice-step end inside the run and at the run's end, over the rows
+// of all G threads. The threads of a run take every branch together (the
+// step tests depend on the position only, and the decisions at
+// lattice-step ends are combined), so their shuffles always pair up. (The
+// run's end is read from shared memory, which keeps it out of the
+// registers the walk state needs.)
+template <int DIM, int NAX, int PM, int QM, class A, int NT, int R, int G>
+__device__ __forceinline__ void walk_axis_range(typename A::T (&m)[R][DIM], int (&ex)[R], const SmemPos<NT> &pos,
+                                                const LevelPlan &L, const StepConst &K, long long alo,
+                                                const long long *ahi, unsigned long long *fail) {
+    if (alo >= *ahi) return;
+    volatile unsigned long long *vf = fail;
+    int skip = (int)(alo % L.L);  // axis steps of the first lattice step before the run
+    long long a = alo - skip;
+    while (true) {
+        for (int i = 0; i < L.k; ++i) {
+            const uint32_t lm = L.mask[i];
+            const int lo = L.thr[i + 1];
+            for (int level = L.thr[i]; level > lo; --level) {
+                uint32_t mask = lm;
+                while (mask) {
+                    const int axis = top_axis(mask);
+                    mask &= ~(1u << axis);
+                    const bool up = (L.up >> axis) & 1u;
+                    if (a >= *ahi) goto run_end;
+                    if (skip > 0) {
+                        pos_move<NAX>(pos, axis, up ? 1.0 : -1.0);
+                        --skip;
+                    } else {
+                        const int st = axis_step<DIM, NAX, PM, QM, A>(m, ex, pos, axis, up, K);
+                        if (st != CMFW_TRAJ_OK) {
+                            atomicMin(fail, fail_key(a, st));
+                            return;
+                        }
+                    }
+                    ++a;
+                }
+            }
+        }
+        {
+            // (an identity, before the run's first step, is healthy)
+            int bits = health_bits<A, R, DIM>(m) | (*vf < fail_key(a, 0) ? 4 : 0);
+            if (G == 2) bits |= __shfl_xor_sync(pair_mask(), bits, 1);
+            if (!(bits & 1) || (bits & 2)) {
+                atomicMin(fail, fail_key(a - 1, CMFW_TRAJ_NONFINITE));
+                return;
+            }
+            if (a >= *ahi || (bits & 4)) return;  // run done, or an earlier axis step failed
+        }
+    }
+run_end:
+    int bits = health_bits<A, R, DIM>(m);
+    if (G == 2) bits |= __shfl_xor_sync(pair_mask(), bits, 1);
+    if (!(bits & 1) || (bits & 2)) atomicMin(fail, fail_key(a - 1, CMFW_TRAJ_NONFINITE));
+}
+
+// A run's rows (row r * G + h of the walk in this thread's row r) in
+// matrix-exponent form: the largest row exponent among non-zero rows of
+// the G threads becomes the matrix exponent (returned), rows more than
+// 2^1000 below it flush to zero, and each thread writes its rows to out.
+template <int DIM, int R, int G, class A>
+__device__ __forceinline__ int rows_to_matrix_exponent(const typename A::T (&m)[R][DIM], const int (&ex)[R], int h,
+                                                       typename A::Combine::T *out /* DIM*DIM */) {
+    typedef typename A::Combine C;
+    int emax = -0x40000000;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        bool nz = false;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) nz |= A::nonzero(m[r][j]);
+        if (nz && r * G + h < DIM) emax = max(emax, ex[r]);
+    }
+    if (G == 2) emax = max(emax, __shfl_xor_sync(pair_mask(), emax, 1));
+    if (emax == -0x40000000) emax = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int rg = r * G + h;
+        if (rg < DIM) {
+            const int be = max(emax - ex[r], 0);
+            const bool keep = be < 1000;
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) {
+                typename C::T v = A::to_combine(m[r][j]);
+                out[rg * DIM + j] = keep ? C::scale(v, be) : C::from(0.0);
+            }
+        }
+    }
+    return emax;
+}
+
+// CTAs that walk one trajectory together, at most.
+constexpr int kMaxParts = 8;
+
+__device__ __forceinline__ double ldcg_d(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ dd ldcg_d(const dd *p) { return dd{__ldcg(&p->hi), __ldcg(&p->lo)}; }
 
 template <int P_, int Q_, int DIM, class A>
-__global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArgs C) {
+__global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(ChunkArgs C) {
     constexpr int NT = chunk_threads(DIM);
-    constexpr int CL = kChunkCluster;
+    constexpr int G = chunk_pair(DIM);   // threads per run
+    constexpr int RT = NT / G;           // runs (product slots) per CTA
+    constexpr int R = (DIM + G - 1) / G; // walk rows per thread
     typedef typename A::T T;
     typedef typename A::Combine CA;
     typedef typename CA::T CT;
@@ -197,240 +353,273 @@ __global__ void __launch_bounds__(chunk_threads(DIM)) walk_chunk_kernel(ChunkArg
     constexpr int QM = (P_ > 0) ? Q_ : 7;
     constexpr int DD = DIM * DIM;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    CT *smem = (CT *)smem_raw;                  // NT run products + 6 work matrices
-    int *sexp = (int *)(smem + (NT + 6) * DD);  // NT + 6 exponents
-    ProdTask<CA> *tasks = (ProdTask<CA> *)(((uintptr_t)(sexp + NT + 6) + 15) & ~(uintptr_t)15);  // NT / 2
-    int *pmax = (int *)(tasks + NT / 2);        // NT / 2
-    unsigned char *ureg = smem_raw + (chunk_union_offset<CT>(DIM, NT) + 15) / 16 * 16;
+    CT *smem = (CT *)smem_raw;                  // RT run products + 3 snapshot matrices
+    int *sexp = (int *)(smem + (RT + 3) * DD);  // RT + 3 exponents
+    ProdTask<CA> *tasks = (ProdTask<CA> *)(((uintptr_t)(sexp + RT + 3) + 15) & ~(uintptr_t)15);  // RT / 2
+    int *pmax = (int *)(tasks + RT / 2);        // RT / 2
+    unsigned char *ureg = smem_raw + (chunk_union_offset<CT>(DIM) + 15) / 16 * 16;
     double *s_pos = (double *)ureg;             // during the runs: [NAX][NT] positions
     CT *stage = (CT *)ureg;                     // afterwards: product staging
-    __shared__ int s_ntask, s_fkey, s_ok;
+    __shared__ int s_ntask, s_ok, s_last;
     __shared__ double s_ls[3];
-    // earliest failing lattice step of this CTA's runs, as step * 16 + status
-    __shared__ int s_fail;
+    // earliest failing axis step of this CTA's runs (fail_key), and of the
+    // trajectory once the parts are combined
+    __shared__ unsigned long long s_fail, s_fkey;
     __shared__ LevelPlan s_plan;
-    cg::cluster_group cluster = cg::this_cluster();
-    const int crank = (int)cluster.block_rank();
+    // groups of shared-memory products for group_products
+    __shared__ int s_gbase[3], s_gcnt[3];
+    __shared__ StepConst s_K;
+    __shared__ long long s_ahi[NT];  // each thread's run end
+    __shared__ int s_t;  // the trajectory walked
     const int tid = threadIdx.x;
     const int P = (P_ > 0) ? P_ : W.p;
     const int Q = (P_ > 0) ? Q_ : W.q;
     const int naxes = P + Q;
-    const StepConst K = make_step_const(P, Q, DIM, W.z);
+    if (tid == 0) s_K = make_step_const(P, Q, DIM, W.z);
 
     // parts per trajectory: as many CTAs as the survivors leave room for
-    const int count = *C.count;
-    const int nclusters = gridDim.x / CL;
-    const int NP = (count * CL <= (int)gridDim.x) ? CL : 1;
-    const int per_cluster = CL / NP;
-    const int part = crank % NP, sub = crank / NP;
-    const int NTOT = NT * NP;
-
-    // segments of lattice steps and the runs (global index g over the NP
-    // CTAs) that cover them; the same for every trajectory of the launch.
-    // Kept in shared memory and re-derived where needed, so that none of it
-    // holds a register across the runs.
-    __shared__ int s_segbase[3], s_segT[3];
+    // (kept in shared memory, like the other per-launch values below)
+    __shared__ int s_count, s_np;
     if (tid == 0) {
-        const int rest = W.N;
-        int T1 = (NTOT * W.h + rest / 2) / rest;
-        T1 = max(1, min(T1, W.h));
-        const int T2 = max(1, min(T1, W.h));
-        const int T0 = NTOT - T1 - T2;
-        s_segbase[0] = 0;
-        s_segbase[1] = T0;
-        s_segbase[2] = T0 + T1;
-        s_segT[0] = T0;
-        s_segT[1] = T1;
-        s_segT[2] = T2;
+        const int count = *C.count;
+        s_count = count;
+        s_np = count > 0 ? max(1, min(kMaxParts, min((int)gridDim.x, C.nslots) / count)) : 1;
     }
     __syncthreads();
-    const int g = part * NT + tid;
 
-    for (int round = 0;; ++round) {
-        const int b0 = (round * nclusters + (int)(blockIdx.x / CL)) * per_cluster;
-        if (b0 >= count) break;  // uniform over the cluster
-        const int b = b0 + sub;
-        const bool active = b < count;
-        const int t = active ? C.list[b] : 0;
-        if (tid == 0) {
-            s_fail = 0x7fffffff;
-            if (active) {
-                int absd[NAX];
-                uint32_t neg;
-                const int maxabs = load_direction<NAX>(W.in[t], naxes, absd, neg);
-                make_level_plan<NAX>(absd, neg, maxabs, s_plan);
+    // The walk's three segments of lattice steps [1, N-2h], [N-2h+1, N-h],
+    // [N-h+1, N] (their ends are the snapshot depths) are tiled by blocks of
+    // x lattice steps (a segment's last block may be shorter), and every
+    // block is cut into c pieces at the same axis-step offsets: piece i of a
+    // block covers axis steps floor(i x L / c) .. floor((i+1) x L / c) of it
+    // (L = sum |dir|). One piece is one thread's run. Piece i of every block
+    // goes to warps of its own, so the threads of a warp start their runs at
+    // the same offset inside a lattice step and walk the same number of axis
+    // steps: no divergence. Runs are numbered block by block (run j = piece
+    // j % c of block j / c), part p holds runs [p NT, (p+1) NT) and puts run
+    // j's product in shared slot j - p RT, so a segment's runs sit in
+    // consecutive slots in walk order. (c, x) minimise the run length x / c
+    // over the blocks the NP parts can hold. The same for every trajectory
+    // of the launch; kept in shared memory and re-derived where needed, so
+    // that none of it holds a register across the runs.
+    __shared__ int s_c, s_x, s_blockbase[3], s_segbase[3], s_segT[3];
+    if (tid == 0) {
+        const int n[3] = {W.N - 2 * W.h, W.h, W.h};
+        int best_c = 1, best_x = 1 << 30;
+        for (int c = 1; c <= 8 && (RT / c) * G >= 32; c <<= 1) {
+            const int cap = s_np * (RT / c);
+            int x = max(1, (W.N + cap - 1) / cap);
+            while ((n[0] + x - 1) / x + (n[1] + x - 1) / x + (n[2] + x - 1) / x > cap) ++x;
+            if ((long long)x * best_c < (long long)best_x * c) {
+                best_c = c;
+                best_x = x;
             }
         }
-        T m[DIM][DIM];
-        int ex[DIM];
+        s_c = best_c;
+        s_x = best_x;
+        int bb = 0;
+        for (int k = 0; k < 3; ++k) {
+            const int nb = (n[k] + best_x - 1) / best_x;
+            s_blockbase[k] = bb;
+            s_segbase[k] = bb * best_c;
+            s_segT[k] = nb * best_c;
+            bb += nb;
+        }
+    }
+    __syncthreads();
+
+    for (int u = blockIdx.x;; u += gridDim.x) {
+        if (u / s_np >= s_count) break;  // uniform over the CTA
+        if (tid == 0) {
+            const int t = C.list[u / s_np];
+            s_t = t;
+            s_fail = kNoFailure;
+            int absd[NAX];
+            uint32_t neg;
+            const int maxabs = load_direction<NAX>(W.in[t], naxes, absd, neg);
+            make_level_plan<NAX>(absd, neg, maxabs, s_plan);
+        }
+        // this thread's rows of the walk (row r * G + h in row r; a row past
+        // DIM, in the second thread of a pair at odd rank, stays zero)
+        T m[R][DIM];
+        int ex[R];
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) {
+        for (int r = 0; r < R; ++r) {
             ex[r] = 0;
 #pragma unroll
-            for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r == j) ? 1.0 : 0.0);
+            for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r * G + tid % G == j) ? 1.0 : 0.0);
         }
         __syncthreads();
-        if (active) {
-            // this thread's run [lo, hi) of lattice steps
-            const int seg = g < s_segbase[1] ? 0 : (g < s_segbase[2] ? 1 : 2);
-            const int Lseg = seg == 0 ? W.N - 2 * W.h : W.h;
-            const int first = seg == 0 ? 1 : (seg == 1 ? W.N - 2 * W.h + 1 : W.N - W.h + 1);
-            const int local = g - s_segbase[seg];
-            const int lo = first + (int)(((long long)local * Lseg) / s_segT[seg]);
-            const int hi = first + (int)(((long long)(local + 1) * Lseg) / s_segT[seg]);
-            const cmfw_traj_in &in = W.in[t];
+        {
+            // this thread's run: piece i of block B
+            const int NB = RT / s_c, v = tid / G;
+            const int B = (u % s_np) * NB + v % NB, i = v / NB;
+            const int k = B < s_blockbase[1] ? 0 : (B < s_blockbase[2] ? 1 : 2);
+            const int nk = k == 0 ? W.N - 2 * W.h : W.h;
+            const int first = k == 0 ? 1 : (k == 1 ? W.N - 2 * W.h + 1 : W.N - W.h + 1);
+            const int sb = first + (B - s_blockbase[k]) * s_x;  // the block's first lattice step
+            const int se = min(sb + s_x, first + nk);            // one past its last
+            const long long Lk = s_plan.L;
+            const long long b0 = (long long)(sb - 1) * Lk;
+            long long alo = b0 + (long long)i * s_x * Lk / s_c;
+            long long ahi = min(b0 + (long long)(i + 1) * s_x * Lk / s_c, (long long)(se - 1) * Lk);
+            if (sb >= first + nk) alo = ahi = 0;  // beyond the last block: no run
+            s_ahi[tid] = ahi;
+            const cmfw_traj_in &in = W.in[s_t];
             const SmemPos<NT> pos{s_pos + tid};
+            // lattice steps completed before the run (a zero direction has
+            // no axis steps: every run is empty)
+            const double s0 = Lk > 0 ? (double)(alo / Lk) : 0.0;
 #pragma unroll
             for (int a = 0; a < NAX; ++a) {
                 const double d = (a < naxes) ? (double)in.dir[a] : 0.0;
-                pos.p[a * NT] = (a < naxes) ? in.start[a] + (double)(lo - 1) * d : 0.0;
+                pos.p[a * NT] = (a < naxes) ? in.start[a] + s0 * d : 0.0;
             }
-            volatile int *fail = &s_fail;
-            for (int step = lo; step < hi; ++step) {
-                if (*fail < step * 16) break;  // an earlier step failed: this run is moot
-                int st = lattice_step_plan<DIM, NAX, PM, QM, A>(m, ex, pos, s_plan, K);
-                if (st == CMFW_TRAJ_OK && !healthy<A, DIM>(m)) st = CMFW_TRAJ_NONFINITE;
-                if (st != CMFW_TRAJ_OK) {
-                    atomicMin(&s_fail, step * 16 + st);
-                    break;
+            walk_axis_range<DIM, NAX, PM, QM, A, NT, R, G>(m, ex, pos, s_plan, s_K, alo, s_ahi + tid, &s_fail);
+        }
+        {
+            const int NB = RT / s_c, v = tid / G;
+            const int slot = (v % NB) * s_c + v / NB;
+            const int e = rows_to_matrix_exponent<DIM, R, G, A>(m, ex, tid % G, smem + slot * DD);
+            if (tid % G == 0) sexp[slot] = e;
+        }
+        const int b = u / s_np, part = u % s_np;
+        if (tid == 0) {
+            // this CTA's share of each segment's runs, in shared slots
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int b0 = max(s_segbase[k], part * RT);
+                const int b1 = min(s_segbase[k] + s_segT[k], (part + 1) * RT);
+                s_gbase[k] = b0 - part * RT;
+                s_gcnt[k] = max(0, b1 - b0);
+            }
+        }
+        __syncthreads();
+        // in-order tree product of this CTA's runs of each segment
+        group_products<DIM, CA, NT>(smem, sexp, s_gbase, s_gcnt, tasks, pmax, stage, &s_ntask);
+
+        const int NP = s_np;
+        if (NP > 1) {
+            // publish this part's segment products; the last part to
+            // finish combines them (no CTA waits for another)
+            const size_t slot = (size_t)b * NP + part;
+            CT *pp = (CT *)C.parts + slot * 3 * DD;
+            for (int i = tid; i < 3 * DD; i += NT) {
+                const int k = i / DD;
+                if (s_gcnt[k] > 0) pp[i] = smem[s_gbase[k] * DD + i % DD];
+            }
+            if (tid < 3 && s_gcnt[tid] > 0) C.parts_e[slot * 3 + tid] = sexp[s_gbase[tid]];
+            if (tid == 0) C.parts_fail[slot] = s_fail;
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = atomicAdd(&C.arrive[b], 1) == NP - 1;
+            __syncthreads();
+            if (!s_last) continue;  // uniform over the CTA
+            __threadfence();
+            if (tid == 0) {
+                unsigned long long fk = kNoFailure;
+                for (int q = 0; q < NP; ++q) fk = min(fk, __ldcg(&C.parts_fail[(size_t)b * NP + q]));
+                s_fkey = fk;
+                // segment k's products are those of parts q0 .. q1, in order
+                int at = 0;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const int q0 = s_segbase[k] / RT, q1 = (s_segbase[k] + s_segT[k] - 1) / RT;
+                    s_gbase[k] = at;
+                    s_gcnt[k] = q1 - q0 + 1;
+                    at += q1 - q0 + 1;
                 }
             }
-        }
-        sexp[tid] = to_matrix_exponent<DIM, A>(m, ex, smem + tid * DD);
-        __syncthreads();
-        // this CTA's share of its segment's runs: lrel = index among them,
-        // ccnt = their number
-        int lrel, ccnt;
-        {
-            const int seg = g < s_segbase[1] ? 0 : (g < s_segbase[2] ? 1 : 2);
-            const int b0 = max(s_segbase[seg], part * NT);
-            const int b1 = min(s_segbase[seg] + s_segT[seg], (part + 1) * NT);
-            lrel = tid - (b0 - part * NT);
-            ccnt = max(0, b1 - b0);
-        }
-        // in-order tree product of this CTA's runs of each segment, one
-        // level at a time, every level's products spread over the CTA
-        for (int stride = 1; stride < NT; stride <<= 1) {
-            if (tid == 0) s_ntask = 0;
             __syncthreads();
-            if (active && (lrel % (2 * stride)) == 0 && lrel + stride < ccnt) {
-                const int q = atomicAdd(&s_ntask, 1);
-                tasks[q] = ProdTask<CA>{smem + tid * DD, smem + (tid + stride) * DD, smem + tid * DD, sexp[tid],
-                                        sexp[tid + stride], &sexp[tid]};
-                pmax[q] = 0;
+            if (s_fkey == kNoFailure) {
+                const int nslot = s_gbase[2] + s_gcnt[2];
+                for (int i = tid; i < nslot * DD; i += NT) {
+                    const int sl = i / DD;
+                    const int k = sl < s_gbase[1] ? 0 : (sl < s_gbase[2] ? 1 : 2);
+                    const int q = s_segbase[k] / RT + (sl - s_gbase[k]);
+                    const size_t src = ((size_t)b * NP + q) * 3 + k;
+                    smem[i] = ldcg_d((const CT *)C.parts + src * DD + i % DD);
+                    if (i % DD == 0) sexp[sl] = __ldcg(&C.parts_e[src]);
+                }
+                __syncthreads();
+                group_products<DIM, CA, NT>(smem, sexp, s_gbase, s_gcnt, tasks, pmax, stage, &s_ntask);
             }
+        } else {
+            if (tid == 0) s_fkey = s_fail;
             __syncthreads();
-            const int nt = s_ntask;
-            if (nt == 0) break;  // no segment has runs this far apart
-            par_products<DIM, CA, NT>(tasks, nt, pmax, stage);
         }
-        // every part's products and failure key are final (CTAs that walk
-        // alone need no cluster barrier)
-        if (NP > 1) cluster.sync();
-        if (active && part == 0) {
-            // the leader CTA combines the parts in order, forms the snapshots
-            // and reduces them
-            CT *y = smem + NT * DD, *x = y + 3 * DD;
-            int *ye = sexp + NT, *xe = ye + 3;
+
+        // the combined trajectory: segment products in slots s_gbase[k]
+        const int t = s_t;
+        CT *x = smem + RT * DD;
+        int *xe = sexp + RT;
+        if (s_fkey != kNoFailure) {
+            if (tid == 0) write_invalid(W, t, (int)(s_fkey & 15));
+        } else {
+            // snapshots: seg0, then * seg1, then * seg2
+            for (int i = tid; i < DD; i += NT) x[i] = smem[s_gbase[0] * DD + i];
             if (tid == 0) {
-                int fkey = 0x7fffffff;
-                for (int q = 0; q < NP; ++q) fkey = min(fkey, *cluster.map_shared_rank(&s_fail, crank + q));
-                s_fkey = fkey;
-                s_ntask = 0;
+                xe[0] = sexp[s_gbase[0]];
                 s_ok = 1;
             }
             __syncthreads();
-            if (s_fkey != 0x7fffffff) {
-                if (tid == 0) write_invalid(W, t, s_fkey & 15);
+            for (int k = 1; k < 3; ++k) {
+                if (tid == 0) {
+                    tasks[0] = ProdTask<CA>{x + (k - 1) * DD, smem + s_gbase[k] * DD, x + k * DD, xe[k - 1],
+                                            sexp[s_gbase[k]], &xe[k]};
+                    pmax[0] = 0;
+                }
+                __syncthreads();
+                par_products<DIM, CA, NT>(tasks, 1, pmax, stage);
+            }
+            double *snap = W.snap + (size_t)t * 3 * DD;
+            int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
+            for (int i = tid; i < 3 * DD; i += NT) {
+                const double v = CA::to(x[i]);
+                snap[i] = v;
+                if (!isfinite(v)) atomicAnd(&s_ok, 0);
+            }
+            if (tid < 3 * DIM) snap_e[tid] = xe[tid / DIM];
+            __syncthreads();
+            if (tid < 3) {
+                bool nz = false;
+                for (int i = 0; i < DD; ++i) nz |= snap[tid * DD + i] != 0.0;
+                if (!nz) atomicAnd(&s_ok, 0);
+            }
+            __syncthreads();
+            if (!s_ok) {
+                if (tid == 0) write_invalid(W, t, CMFW_TRAJ_NONFINITE);
             } else {
-                // segment k = first part's product [* second part's product]
-                if (tid < 3) {
-                    const int k = tid;
-                    const CT *pm[2];
-                    int pe[2], np = 0;
-                    for (int q = 0; q < NP; ++q) {
-                        const int b0q = max(s_segbase[k], q * NT), b1q = min(s_segbase[k] + s_segT[k], (q + 1) * NT);
-                        if (b1q <= b0q) continue;
-                        const int slot = b0q - q * NT;
-                        pm[np] = cluster.map_shared_rank(smem, crank + q) + slot * DD;
-                        pe[np] = *cluster.map_shared_rank(sexp + slot, crank + q);
-                        ++np;
-                    }
-                    if (np == 1) {
-                        for (int i = 0; i < DD; ++i) y[k * DD + i] = pm[0][i];
-                        ye[k] = pe[0];
-                    } else {
-                        const int q = atomicAdd(&s_ntask, 1);
-                        tasks[q] = ProdTask<CA>{pm[0], pm[1], y + k * DD, pe[0], pe[1], &ye[k]};
-                        pmax[q] = 0;
-                    }
+                if (tid < 3) s_ls[tid] = normalise_rows(snap + tid * DD, snap_e + tid * DIM, DIM, 0.0);
+                __syncthreads();
+                // limit candidates in parallel, then the in-order selection
+                const int NK = n_limit_candidates(DIM);
+                int *cf = (int *)smem;  // the run products are no longer needed
+                double *cla = (double *)(smem) + NK, *clr = cla + NK;
+                for (int k = tid; k < NK; k += NT) {
+                    double LA = 0.0, LR = 0.0;
+                    cf[k] = limit_candidate(snap, snap + DD, snap + 2 * DD, DIM, k, &LA, &LR);
+                    cla[k] = LA;
+                    clr[k] = LR;
                 }
                 __syncthreads();
-                if (s_ntask > 0) par_products<DIM, CA, NT>(tasks, s_ntask, pmax, stage);
-                // snapshots: seg0, then * seg1, then * seg2
-                for (int i = tid; i < DD; i += NT) x[i] = y[i];
-                if (tid == 0) xe[0] = ye[0];
-                __syncthreads();
-                for (int k = 1; k < 3; ++k) {
-                    if (tid == 0) {
-                        tasks[0] = ProdTask<CA>{x + (k - 1) * DD, y + k * DD, x + k * DD, xe[k - 1], ye[k], &xe[k]};
-                        pmax[0] = 0;
-                    }
-                    __syncthreads();
-                    par_products<DIM, CA, NT>(tasks, 1, pmax, stage);
-                }
-                double *snap = W.snap + (size_t)t * 3 * DD;
-                int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
-                for (int i = tid; i < 3 * DD; i += NT) {
-                    const double v = CA::to(x[i]);
-                    snap[i] = v;
-                    if (!isfinite(v)) atomicAnd(&s_ok, 0);
-                }
-                if (tid < 3 * DIM) snap_e[tid] = xe[tid / DIM];
-                __syncthreads();
-                if (tid < 3) {
-                    bool nz = false;
-                    for (int i = 0; i < DD; ++i) nz |= snap[tid * DD + i] != 0.0;
-                    if (!nz) atomicAnd(&s_ok, 0);
-                }
-                __syncthreads();
-                if (!s_ok) {
-                    if (tid == 0) write_invalid(W, t, CMFW_TRAJ_NONFINITE);
-                } else {
-                    if (tid < 3) s_ls[tid] = normalise_rows(snap + tid * DD, snap_e + tid * DIM, DIM, 0.0);
-                    __syncthreads();
-                    // limit candidates in parallel, then the in-order selection
-                    const int K = n_limit_candidates(DIM);
-                    int *cf = (int *)smem;                     // run products are no longer needed
-                    double *cla = (double *)(smem) + K, *clr = cla + K;
-                    for (int k = tid; k < K; k += NT) {
-                        double LA = 0.0, LR = 0.0;
-                        cf[k] = limit_candidate(snap, snap + DD, snap + 2 * DD, DIM, k, &LA, &LR);
-                        cla[k] = LA;
-                        clr[k] = LR;
-                    }
-                    __syncthreads();
-                    if (tid == 0) {
-                        LimitScan scn;
-                        for (int k = 0; k < K; ++k)
-                            if (cf[k]) scn.add(cf[k], cla[k], clr[k], k, DIM);
-                        cmfw_traj_out o;
-                        o.valid = 1;
-                        o.n_limits = scn.n;
-                        o.limit = scn.have_aitken ? scn.first_aitken : (scn.n > 0 ? scn.first_any : (double)NAN);
-                        reduce_tail(snap, DIM, s_ls, o.limit, o);
-                        W.out[t] = o;
-                        if (W.status) W.status[t] = CMFW_TRAJ_OK;
-                        if (W.limit_src)
-                            W.limit_src[t] = scn.have_aitken ? scn.src_aitken : (scn.n > 0 ? scn.src_any : -1);
-                    }
+                if (tid == 0) {
+                    LimitScan scn;
+                    for (int k = 0; k < NK; ++k)
+                        if (cf[k]) scn.add(cf[k], cla[k], clr[k], k, DIM);
+                    cmfw_traj_out o;
+                    o.valid = 1;
+                    o.n_limits = scn.n;
+                    o.limit = scn.have_aitken ? scn.first_aitken : (scn.n > 0 ? scn.first_any : (double)NAN);
+                    reduce_tail(snap, DIM, s_ls, o.limit, o);
+                    W.out[t] = o;
+                    if (W.status) W.status[t] = CMFW_TRAJ_OK;
+                    if (W.limit_src)
+                        W.limit_src[t] = scn.have_aitken ? scn.src_aitken : (scn.n > 0 ? scn.src_any : -1);
                 }
             }
         }
-        if (NP > 1)
-            cluster.sync();  // the leader has read every part's shared memory
-        else
-            __syncthreads();  // shared products are reused by the next trajectory
+        __syncthreads();  // shared memory is reused by the next trajectory
     }
 }
 
@@ -458,61 +647,75 @@ static ChunkPick<A> pick_chunk(int p, int q, int dim) {
     return ChunkPick<A>{nullptr, nullptr, 0};
 }
 
-// Survivor list and counter.
-size_t chunk_scratch_bytes(int dim, int n) {
-    (void)dim;
-    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    return al((size_t)n * sizeof(int)) + 256;
+// Product slots for trajectories walked in parts: one per CTA of the
+// chunk grid, which is never larger.
+static int chunk_slots() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    return 2 * sms;
 }
+
+struct ChunkLayout {
+    size_t list, count, parts, parts_e, parts_fail, total;
+};
+static ChunkLayout chunk_layout(int dim, int n, int nslots) {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    ChunkLayout L;
+    L.list = 0;
+    L.count = al((size_t)n * sizeof(int));
+    L.parts = L.count + al((size_t)(1 + nslots) * sizeof(int));  // count, then arrive[nslots]
+    L.parts_e = L.parts + al((size_t)nslots * 3 * dim * dim * sizeof(dd));
+    L.parts_fail = L.parts_e + al((size_t)nslots * 3 * sizeof(int));
+    L.total = L.parts_fail + al((size_t)nslots * sizeof(unsigned long long));
+    return L;
+}
+
+// Survivor list and counter, arrival counters and the parts' products.
+size_t chunk_scratch_bytes(int dim, int n) { return chunk_layout(dim, n, chunk_slots()).total; }
 
 template <class A>
 static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_steps, cudaStream_t s) {
     ChunkPick<A> k = pick_chunk<A>(W.p, W.q, W.dim);
     if (!k.prefix) return cudaErrorInvalidValue;
-    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const int dim = W.dim, n = W.n_traj;
+    const int nslots = chunk_slots();
+    const ChunkLayout lay = chunk_layout(dim, n, nslots);
+    char *p = (char *)scratch;
     ChunkArgs C;
     C.w = W;
-    char *p = (char *)scratch;
-    C.list = (int *)p;
-    p += al((size_t)n * sizeof(int));
-    C.count = (int *)p;
+    C.list = (int *)(p + lay.list);
+    C.count = (int *)(p + lay.count);
+    C.arrive = C.count + 1;
+    C.parts = p + lay.parts;
+    C.parts_e = (int *)(p + lay.parts_e);
+    C.parts_fail = (unsigned long long *)(p + lay.parts_fail);
+    C.nslots = nslots;
     C.prefix_steps = prefix_steps;
     const int NT = chunk_threads(dim);
-    const size_t shmem = chunk_smem_bytes<typename A::Combine::T>(dim, NT);
+    const size_t shmem = chunk_smem_bytes<typename A::Combine::T>(dim);
     cudaError_t e = cudaFuncSetAttribute((const void *)k.chunk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shmem);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(C.count, 0, sizeof(int), s);
+    e = cudaMemsetAsync(C.count, 0, (size_t)(1 + nslots) * sizeof(int), s);
     if (e != cudaSuccess) return e;
-    k.prefix<<<(n + 127) / 128, 128, 0, s>>>(C);
+    k.prefix<<<(n + kFilterThreads - 1) / kFilterThreads, kFilterThreads, 0, s>>>(C);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    // persistent grid of 2-CTA clusters: as many as can be resident at once
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kChunkCluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(NT, 1, 1);
-    cfg.dynamicSmemBytes = shmem;
-    cfg.stream = s;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int dev = 0, sms = 148;
+    // persistent grid: as many CTAs as can be resident at once, at most
+    // kMaxParts per trajectory and one per product slot
+    int dev = 0, sms = 148, per_sm = 1;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cfg.gridDim = dim3((unsigned)(sms / kChunkCluster * kChunkCluster), 1, 1);
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, (const void *)k.chunk, &cfg) != cudaSuccess || clusters < 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k.chunk, NT, shmem) != cudaSuccess ||
+        per_sm < 1) {
         cudaGetLastError();
-        clusters = sms / kChunkCluster;
+        per_sm = 1;
     }
-    const int need = (n + kChunkCluster - 1) / kChunkCluster;  // one trajectory per CTA at most
-    clusters = max(1, min(clusters, need));
-    cfg.gridDim = dim3((unsigned)(clusters * kChunkCluster), 1, 1);
-    e = cudaLaunchKernelEx(&cfg, k.chunk, C);
-    return e != cudaSuccess ? e : cudaGetLastError();
+    long long grid = (long long)sms * per_sm;
+    grid = std::min<long long>(grid, (long long)std::max(n, 1) * kMaxParts);
+    grid = std::min<long long>(grid, nslots);
+    k.chunk<<<(unsigned)grid, NT, shmem, s>>>(C);
+    return cudaGetLastError();
 }
 
 // ff selects the df64 walk (float-float runs); otherwise the f64 walk with

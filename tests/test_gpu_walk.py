@@ -295,6 +295,40 @@ def test_df64_compat_matches_oracle(cuda):
     np.testing.assert_allclose(g["q"], o["q"], rtol=1e-7)
 
 
+@pytest.mark.parametrize("variant,rtol", [("f64", 1e-11), ("df64", 1e-9)])
+def test_chunk_parts_agree(cuda, variant, rtol):
+    """The chunked walk spreads each survivor over as many CTAs as the batch
+    leaves room for (1 to 8 parts, combined by the last part to finish) and
+    cuts runs inside lattice steps; every batch size gives a different
+    association of the same product. Zeta-start limit walks are well
+    conditioned, so every batch size -- every part count -- must give the
+    oracle's limit, p and q to rtol."""
+    for p, q in [(6, 5), (3, 2), (8, 7)]:
+        recs = oracle.make_inputs(p, q, 200, 0, True)
+        desc = cmfw.make_desc(p, q, 1.0)
+        o = oracle.walk("f64", p, q, 1.0, 1000, 50, recs, fused=True)
+        assert (o["valid"] == 1).all()
+        for n in (1, 3, 20, 40, 60, 200):  # 8, 8, 7, 3, 2 and 1 parts on 148 SMs
+            g = cmfw.walk(variant, desc, recs[:n], 1000, 50)
+            np.testing.assert_array_equal(g["valid"], o["valid"][:n])
+            for k in ("limit", "p", "q"):
+                np.testing.assert_allclose(g[k], o[k][:n], rtol=rtol, atol=0, err_msg=f"{p}F{q} n={n} {k}")
+
+
+def test_zero_direction_walks_nowhere(cuda):
+    """A zero direction has no axis steps: every run of the chunked walk is
+    empty and the snapshots are the identity, as in the oracle."""
+    desc = cmfw.make_desc(3, 2, 0.5)
+    recs = oracle.make_inputs(3, 2, 8, 0, False)[:4].copy()
+    recs["dir"][2, :] = 0
+    o = oracle.walk("f64", 3, 2, 0.5, 200, 20, recs, fused=True)
+    for flags in (0, cmfw.F_SEQUENTIAL):
+        g = cmfw.walk("f64", desc, recs, 200, 20, flags=flags)
+        np.testing.assert_array_equal(g["valid"], o["valid"])
+        for k in ("limit", "p", "q", "log_scale"):
+            np.testing.assert_allclose(g[k], o[k], rtol=1e-12, atol=0, equal_nan=True, err_msg=k)
+
+
 def test_failure_statuses(cuda):
     desc = cmfw.make_desc(3, 2, 0.5)
     recs = oracle.make_inputs(3, 2, 8, 0, False)[:8].copy()
