@@ -15,14 +15,16 @@
 //     solve, which every arithmetic forms the same way), so the verdict is
 //     the run arithmetic's; the survivors' first steps are walked again by
 //     the chunk kernel's runs.
-//  2. chunk: CTAs of NT threads (256 up to rank 6, else 128) on a
-//     persistent grid; each survivor is walked by NP CTAs ("parts"), NP as
-//     large as the survivors leave CTAs for (at most kMaxParts). Steps
+//  2. chunk: CTAs of 256 threads on a grid of one CTA per SM; each
+//     survivor is walked by NP_b CTAs ("parts"), NP_b proportional to its
+//     cost (axis steps per lattice step) so that all CTAs end together (at
+//     most kMaxParts; with more survivors than CTAs, one CTA each). Steps
 //     1..N form three segments [1, N-2h], [N-2h+1, N-h], [N-h+1, N] (the
 //     snapshot depths are segment ends). Every segment's axis steps are
 //     split evenly over its runs, one run per thread, so a run may start
 //     and end inside a lattice step; each thread walks its run with the
-//     same registers-only step as the sequential kernel, and a CTA
+//     same registers-only step as the sequential kernel (from rank 7 two
+//     threads share a run, each holding half the rows), and a CTA
 //     multiplies its runs of each segment in order by a shared-memory
 //     tree. A trajectory walked in parts is finished by the part that
 //     ends last: the parts publish their segment products to global
@@ -30,10 +32,10 @@
 //     ever waits for another) multiplies them in order, forms the three
 //     snapshots seg0, seg0 * seg1, seg0 * seg1 * seg2 and reduces them.
 //
-// The latency of one trajectory drops from N lattice steps to about
-// N * L / (NP * NT) axis steps (L = sum |dir|) + log2 NT + log2 NP matrix
-// products; the total arithmetic is that of the sequential walk plus
-// NP * NT - 1 dense rank^3 products.
+// The latency of one trajectory drops from N L axis steps (L = sum |dir|)
+// to about N L / (NP RT) axis steps (RT runs per CTA) + log2 RT + log2 NP
+// matrix products; the total arithmetic is that of the sequential walk
+// plus NP RT - 1 dense rank^3 products.
 //
 // Accuracy. Multiplying runs together is a different association of the
 // same matrix product. A run started from the identity can pass through
@@ -58,6 +60,7 @@ struct ChunkArgs {
     WalkArgs w;
     int *list;                        // n_traj survivor indices
     int *count;                       // survivors
+    int *cost;                        // n_traj: axis steps per lattice step of each listed survivor
     int *arrive;                      // nslots: parts finished, per survivor walked in parts
     void *parts;                      // nslots x 3 segment products of the parts (combine arithmetic)
     int *parts_e;                     // nslots x 3 their exponents
@@ -99,7 +102,12 @@ __global__ void __launch_bounds__(kFilterThreads) walk_prefix_kernel(ChunkArgs C
         const int st = lattice_step_tests<DIM, NAX, PM, QM>(pos, absd, neg, maxabs, K);
         if (st != CMFW_TRAJ_OK) { write_invalid(W, t, st); return; }
     }
-    C.list[atomicAdd(C.count, 1)] = t;
+    const int at = atomicAdd(C.count, 1);
+    C.list[at] = t;
+    int L = 0;
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) L += absd[a];
+    C.cost[at] = L;
 }
 
 // Threads per CTA of the chunk kernel, and threads per run: up to rank 6 a
@@ -195,33 +203,73 @@ __host__ __device__ constexpr size_t chunk_smem_bytes(int dim) {
 
 // In-order products of up to three groups of consecutive shared-memory
 // matrices (matrix-exponent form): group k holds slots gbase[k] ..
-// gbase[k] + gcnt[k] - 1 and ends with its product in slot gbase[k]. Thread
-// i looks after slot i; every tree level's products are spread over the CTA.
+// gbase[k] + gcnt[k] - 1 and ends with its product in slot gbase[k]. One
+// tree level at a time: at stride st the products are slot a = gbase[k] +
+// 2 st m times slot a + st (for a + st inside the group), enumerated in
+// closed form. Every product's entries take whole warps (DD entries padded
+// to EW = 32 or 64 lanes), each thread ILP entries in flight; a warp's
+// largest exponent is one reduction, and the products are written back
+// rescaled into slot a once every entry is staged. Two barriers a level,
+// no atomics. wmax holds 2 ints per product. (Out of line: its registers
+// are then not counted against the walk state's.)
+__device__ __forceinline__ int level_tasks(int cnt, int st) { return cnt > st ? (cnt - st - 1) / (2 * st) + 1 : 0; }
+
 template <int DIM, class CA, int NT>
-__device__ __forceinline__ void group_products(typename CA::T *slots, int *sexp, const int *gbase, const int *gcnt,
-                                               ProdTask<CA> *tasks, int *pmax, typename CA::T *stage, int *ntask) {
+__device__ __noinline__ void group_products(typename CA::T *slots, int *sexp, const int *gbase, const int *gcnt,
+                                            int *wmax, typename CA::T *stage) {
+    typedef typename CA::T CT;
     constexpr int DD = DIM * DIM;
-    const int tid = threadIdx.x;
-    int rel = -1, cnt = 0;
+    constexpr int EW = 32 * ((DD + 31) / 32);  // lanes per product
+    constexpr int ILP = 4;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int g0 = gbase[0], g1 = gbase[1], g2 = gbase[2];
+    const int c0 = gcnt[0], c1 = gcnt[1], c2 = gcnt[2];
+    const int cmax = max(c0, max(c1, c2));
+    for (int st = 1; st < cmax; st <<= 1) {
+        const int n0 = level_tasks(c0, st), n1 = level_tasks(c1, st), n2 = level_tasks(c2, st);
+        const int nt = n0 + n1 + n2;
+        const int nw = nt * EW;
+#pragma unroll 1
+        for (int w0 = tid; w0 < nw; w0 += ILP * NT) {
+            CT x[ILP];
 #pragma unroll
-    for (int q = 0; q < 3; ++q)
-        if (tid >= gbase[q] && tid < gbase[q] + gcnt[q]) {
-            rel = tid - gbase[q];
-            cnt = gcnt[q];
+            for (int u = 0; u < ILP; ++u) {
+                const int w = w0 + u * NT;  // warp-uniform: nw is a multiple of 32
+                const int tau = w / EW, e = w % EW;
+                if (w < nw && e < DD) {
+                    const int i = e / DIM, j = e % DIM;
+                    const int a = tau < n0 ? g0 + 2 * st * tau
+                                           : (tau < n0 + n1 ? g1 + 2 * st * (tau - n0) : g2 + 2 * st * (tau - n0 - n1));
+                    const CT *A = slots + a * DD, *B = slots + (a + st) * DD;
+                    x[u] = CA::mul(A[i * DIM], B[j]);
+#pragma unroll
+                    for (int k = 1; k < DIM; ++k) x[u] = CA::fma(A[i * DIM + k], B[k * DIM + j], x[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < ILP; ++u) {
+                const int w = w0 + u * NT;
+                if (w < nw) {
+                    const int tau = w / EW, e = w % EW;
+                    const unsigned hx = e < DD ? (unsigned)CA::hexp(x[u]) : 0u;
+                    const unsigned hm = __reduce_max_sync(0xffffffffu, hx);
+                    if (lane == 0) wmax[2 * tau + e / 32] = (int)hm;
+                    if (e < DD) stage[tau * DD + e] = x[u];
+                }
+            }
         }
-    for (int stride = 1; stride < NT; stride <<= 1) {
-        if (tid == 0) *ntask = 0;
         __syncthreads();
-        if (rel >= 0 && (rel % (2 * stride)) == 0 && rel + stride < cnt) {
-            const int q = atomicAdd(ntask, 1);
-            tasks[q] = ProdTask<CA>{slots + tid * DD, slots + (tid + stride) * DD, slots + tid * DD, sexp[tid],
-                                    sexp[tid + stride], &sexp[tid]};
-            pmax[q] = 0;
+#pragma unroll 1
+        for (int w = tid; w < nt * DD; w += NT) {
+            const int tau = w / DD, e = w % DD;
+            const int a = tau < n0 ? g0 + 2 * st * tau
+                                   : (tau < n0 + n1 ? g1 + 2 * st * (tau - n0) : g2 + 2 * st * (tau - n0 - n1));
+            const int hm = EW > 32 ? max(wmax[2 * tau], wmax[2 * tau + 1]) : wmax[2 * tau];
+            const int be = (hm != 0 && hm < 0x7ff00000) ? (hm >> 20) - 1023 : 0;
+            slots[a * DD + e] = CA::scale(stage[w], be);
+            if (e == 0) sexp[a] = sexp[a] + sexp[a + st] + be;
         }
         __syncthreads();
-        const int nt = *ntask;
-        if (nt == 0) break;  // no group has members this far apart
-        par_products<DIM, CA, NT>(tasks, nt, pmax, stage);
     }
 }
 
@@ -332,8 +380,39 @@ __device__ __forceinline__ int rows_to_matrix_exponent(const typename A::T (&m)[
     return emax;
 }
 
-// CTAs that walk one trajectory together, at most.
-constexpr int kMaxParts = 8;
+// The run geometry of a trajectory walked by np parts of rt runs each:
+// blocks of x lattice steps cut into c pieces (see walk_chunk_kernel),
+// with each segment's first block and first run.
+__device__ __forceinline__ void run_geometry(int N, int h, int np, int rt, int g, int *c_out, int *x_out,
+                                          int *blockbase, int *segbase, int *segT) {
+    const int n[3] = {N - 2 * h, h, h};
+    int best_c = 1, best_x = 1 << 30;
+    for (int c = 1; c <= 8 && (rt / c) * g >= 32; c <<= 1) {
+        const int cap = np * (rt / c);
+        int x = max(1, (N + cap - 1) / cap);
+        while ((n[0] + x - 1) / x + (n[1] + x - 1) / x + (n[2] + x - 1) / x > cap) ++x;
+        if ((long long)x * best_c < (long long)best_x * c) {
+            best_c = c;
+            best_x = x;
+        }
+    }
+    *c_out = best_c;
+    *x_out = best_x;
+    int bb = 0;
+    for (int k = 0; k < 3; ++k) {
+        const int nb = (n[k] + best_x - 1) / best_x;
+        blockbase[k] = bb;
+        segbase[k] = bb * best_c;
+        segT[k] = nb * best_c;
+        bb += nb;
+    }
+}
+
+// CTAs that walk one trajectory together, at most, and the survivors per
+// lane of the warp that shares out the parts (32 x 10 covers the largest
+// grid, two CTAs per SM).
+constexpr int kMaxParts = 16;
+constexpr int kLaneItems = 10;
 
 __device__ __forceinline__ double ldcg_d(const double *p) { return __ldcg(p); }
 __device__ __forceinline__ dd ldcg_d(const dd *p) { return dd{__ldcg(&p->hi), __ldcg(&p->lo)}; }
@@ -360,7 +439,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
     unsigned char *ureg = smem_raw + (chunk_union_offset<CT>(DIM) + 15) / 16 * 16;
     double *s_pos = (double *)ureg;             // during the runs: [NAX][NT] positions
     CT *stage = (CT *)ureg;                     // afterwards: product staging
-    __shared__ int s_ntask, s_ok, s_last;
+    __shared__ int s_ok, s_last;
     __shared__ double s_ls[3];
     // earliest failing axis step of this CTA's runs (fail_key), and of the
     // trajectory once the parts are combined
@@ -377,13 +456,64 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
     const int naxes = P + Q;
     if (tid == 0) s_K = make_step_const(P, Q, DIM, W.z);
 
-    // parts per trajectory: as many CTAs as the survivors leave room for
-    // (kept in shared memory, like the other per-launch values below)
-    __shared__ int s_count, s_np;
-    if (tid == 0) {
+    // Parts per trajectory. With no more survivors than CTAs, every
+    // survivor b gets NP_b = min(kMaxParts, ceil(w_b / t)) CTAs, w_b = its
+    // axis steps per lattice step (its walk's cost), t the smallest work
+    // per CTA (in sixteenths) whose parts fit the grid: long walks get more
+    // CTAs, so the CTAs end at about the same time. Survivors take
+    // consecutive CTAs in list order; a CTA walks one part and is done.
+    // With more survivors than CTAs, every survivor is one CTA's and the
+    // CTAs stride over the list. Warp 0 finds this CTA's part; the values
+    // are kept in shared memory, like the run geometry below.
+    __shared__ int s_count, s_bal, s_b0, s_part0, s_np0, s_first0;
+    if (tid < 32) {
         const int count = *C.count;
-        s_count = count;
-        s_np = count > 0 ? max(1, min(kMaxParts, min((int)gridDim.x, C.nslots) / count)) : 1;
+        const int Gr = min((int)gridDim.x, C.nslots);
+        const bool bal = count > 0 && count <= Gr;
+        int b0 = -1, part0 = 0, np0 = 1, first0 = 0;
+        if (bal) {
+            int w[kLaneItems];
+            int wmax = 1;
+#pragma unroll
+            for (int q = 0; q < kLaneItems; ++q) {
+                const int b = tid + 32 * q;
+                w[q] = b < count ? 16 * max(1, C.cost[b]) : 0;
+                wmax = max(wmax, w[q]);
+            }
+            wmax = (int)__reduce_max_sync(0xffffffffu, (unsigned)wmax);
+            int lo = 1, hi = wmax;  // at hi every survivor has one part
+            while (lo < hi) {
+                const int mid = (lo + hi) / 2;
+                int parts = 0;
+#pragma unroll
+                for (int q = 0; q < kLaneItems; ++q)
+                    if (w[q] > 0) parts += min(kMaxParts, (w[q] + mid - 1) / mid);
+                parts = (int)__reduce_add_sync(0xffffffffu, (unsigned)parts);
+                if (parts <= Gr) hi = mid; else lo = mid + 1;
+            }
+            if (tid == 0) {
+                int at = 0;
+                for (int b = 0; b < count; ++b) {
+                    const int np = min(kMaxParts, (16 * max(1, C.cost[b]) + lo - 1) / lo);
+                    if ((int)blockIdx.x < at + np) {
+                        b0 = b;
+                        part0 = blockIdx.x - at;
+                        np0 = np;
+                        first0 = at;
+                        break;
+                    }
+                    at += np;
+                }
+            }
+        }
+        if (tid == 0) {
+            s_count = count;
+            s_bal = bal;
+            s_b0 = b0;
+            s_part0 = part0;
+            s_np0 = np0;
+            s_first0 = first0;
+        }
     }
     __syncthreads();
 
@@ -396,49 +526,44 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
     // goes to warps of its own, so the threads of a warp start their runs at
     // the same offset inside a lattice step and walk the same number of axis
     // steps: no divergence. Runs are numbered block by block (run j = piece
-    // j % c of block j / c), part p holds runs [p NT, (p+1) NT) and puts run
+    // j % c of block j / c), part p holds runs [p RT, (p+1) RT) and puts run
     // j's product in shared slot j - p RT, so a segment's runs sit in
     // consecutive slots in walk order. (c, x) minimise the run length x / c
-    // over the blocks the NP parts can hold. The same for every trajectory
-    // of the launch; kept in shared memory and re-derived where needed, so
-    // that none of it holds a register across the runs.
+    // over the blocks the trajectory's NP parts can hold. Kept in shared
+    // memory and re-derived where needed, so that none of it holds a
+    // register across the runs.
     __shared__ int s_c, s_x, s_blockbase[3], s_segbase[3], s_segT[3];
-    if (tid == 0) {
-        const int n[3] = {W.N - 2 * W.h, W.h, W.h};
-        int best_c = 1, best_x = 1 << 30;
-        for (int c = 1; c <= 8 && (RT / c) * G >= 32; c <<= 1) {
-            const int cap = s_np * (RT / c);
-            int x = max(1, (W.N + cap - 1) / cap);
-            while ((n[0] + x - 1) / x + (n[1] + x - 1) / x + (n[2] + x - 1) / x > cap) ++x;
-            if ((long long)x * best_c < (long long)best_x * c) {
-                best_c = c;
-                best_x = x;
+    // the part this CTA walks: trajectory list index, part, parts, and the
+    // product slot of part 0
+    __shared__ int s_ub, s_upart, s_unp, s_ufirst;
+
+    for (int round = 0;; ++round) {
+        if (tid == 0) {
+            if (s_bal) {
+                s_ub = round == 0 ? s_b0 : -1;
+                s_upart = s_part0;
+                s_unp = s_np0;
+                s_ufirst = s_first0;
+            } else {
+                const int b = blockIdx.x + round * gridDim.x;
+                s_ub = b < s_count ? b : -1;
+                s_upart = 0;
+                s_unp = 1;
+                s_ufirst = 0;
+            }
+            if (s_ub >= 0) {
+                const int t = C.list[s_ub];
+                s_t = t;
+                s_fail = kNoFailure;
+                int absd[NAX];
+                uint32_t neg;
+                const int maxabs = load_direction<NAX>(W.in[t], naxes, absd, neg);
+                make_level_plan<NAX>(absd, neg, maxabs, s_plan);
+                run_geometry(W.N, W.h, s_unp, RT, G, &s_c, &s_x, s_blockbase, s_segbase, s_segT);
             }
         }
-        s_c = best_c;
-        s_x = best_x;
-        int bb = 0;
-        for (int k = 0; k < 3; ++k) {
-            const int nb = (n[k] + best_x - 1) / best_x;
-            s_blockbase[k] = bb;
-            s_segbase[k] = bb * best_c;
-            s_segT[k] = nb * best_c;
-            bb += nb;
-        }
-    }
-    __syncthreads();
-
-    for (int u = blockIdx.x;; u += gridDim.x) {
-        if (u / s_np >= s_count) break;  // uniform over the CTA
-        if (tid == 0) {
-            const int t = C.list[u / s_np];
-            s_t = t;
-            s_fail = kNoFailure;
-            int absd[NAX];
-            uint32_t neg;
-            const int maxabs = load_direction<NAX>(W.in[t], naxes, absd, neg);
-            make_level_plan<NAX>(absd, neg, maxabs, s_plan);
-        }
+        __syncthreads();
+        if (s_ub < 0) break;  // uniform over the CTA
         // this thread's rows of the walk (row r * G + h in row r; a row past
         // DIM, in the second thread of a pair at odd rank, stays zero)
         T m[R][DIM];
@@ -453,7 +578,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
         {
             // this thread's run: piece i of block B
             const int NB = RT / s_c, v = tid / G;
-            const int B = (u % s_np) * NB + v % NB, i = v / NB;
+            const int B = s_upart * NB + v % NB, i = v / NB;
             const int k = B < s_blockbase[1] ? 0 : (B < s_blockbase[2] ? 1 : 2);
             const int nk = k == 0 ? W.N - 2 * W.h : W.h;
             const int first = k == 0 ? 1 : (k == 1 ? W.N - 2 * W.h + 1 : W.N - W.h + 1);
@@ -483,7 +608,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
             const int e = rows_to_matrix_exponent<DIM, R, G, A>(m, ex, tid % G, smem + slot * DD);
             if (tid % G == 0) sexp[slot] = e;
         }
-        const int b = u / s_np, part = u % s_np;
+        const int b = s_ub, part = s_upart;
         if (tid == 0) {
             // this CTA's share of each segment's runs, in shared slots
 #pragma unroll
@@ -496,13 +621,13 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
         }
         __syncthreads();
         // in-order tree product of this CTA's runs of each segment
-        group_products<DIM, CA, NT>(smem, sexp, s_gbase, s_gcnt, tasks, pmax, stage, &s_ntask);
+        group_products<DIM, CA, NT>(smem, sexp, s_gbase, s_gcnt, (int *)tasks, stage);
 
-        const int NP = s_np;
+        const int NP = s_unp;
         if (NP > 1) {
             // publish this part's segment products; the last part to
             // finish combines them (no CTA waits for another)
-            const size_t slot = (size_t)b * NP + part;
+            const size_t slot = (size_t)s_ufirst + part;
             CT *pp = (CT *)C.parts + slot * 3 * DD;
             for (int i = tid; i < 3 * DD; i += NT) {
                 const int k = i / DD;
@@ -514,11 +639,11 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
             __syncthreads();
             if (tid == 0) s_last = atomicAdd(&C.arrive[b], 1) == NP - 1;
             __syncthreads();
-            if (!s_last) continue;  // uniform over the CTA
+            if (!s_last) break;  // uniform over the CTA; a part is a CTA's only work
             __threadfence();
             if (tid == 0) {
                 unsigned long long fk = kNoFailure;
-                for (int q = 0; q < NP; ++q) fk = min(fk, __ldcg(&C.parts_fail[(size_t)b * NP + q]));
+                for (int q = 0; q < NP; ++q) fk = min(fk, __ldcg(&C.parts_fail[(size_t)s_ufirst + q]));
                 s_fkey = fk;
                 // segment k's products are those of parts q0 .. q1, in order
                 int at = 0;
@@ -537,12 +662,12 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
                     const int sl = i / DD;
                     const int k = sl < s_gbase[1] ? 0 : (sl < s_gbase[2] ? 1 : 2);
                     const int q = s_segbase[k] / RT + (sl - s_gbase[k]);
-                    const size_t src = ((size_t)b * NP + q) * 3 + k;
+                    const size_t src = ((size_t)s_ufirst + q) * 3 + k;
                     smem[i] = ldcg_d((const CT *)C.parts + src * DD + i % DD);
                     if (i % DD == 0) sexp[sl] = __ldcg(&C.parts_e[src]);
                 }
                 __syncthreads();
-                group_products<DIM, CA, NT>(smem, sexp, s_gbase, s_gcnt, tasks, pmax, stage, &s_ntask);
+                group_products<DIM, CA, NT>(smem, sexp, s_gbase, s_gcnt, (int *)tasks, stage);
             }
         } else {
             if (tid == 0) s_fkey = s_fail;
@@ -572,8 +697,10 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
                 __syncthreads();
                 par_products<DIM, CA, NT>(tasks, 1, pmax, stage);
             }
-            double *snap = W.snap + (size_t)t * 3 * DD;
-            int *snap_e = W.snap_e + (size_t)t * 3 * DIM;
+            // the snapshots in the reference's form, in shared memory (the
+            // staging area is free once the products are done)
+            double *snap = (double *)stage;
+            int *snap_e = (int *)(snap + 3 * DD);
             for (int i = tid; i < 3 * DD; i += NT) {
                 const double v = CA::to(x[i]);
                 snap[i] = v;
@@ -657,13 +784,14 @@ static int chunk_slots() {
 }
 
 struct ChunkLayout {
-    size_t list, count, parts, parts_e, parts_fail, total;
+    size_t list, cost, count, parts, parts_e, parts_fail, total;
 };
 static ChunkLayout chunk_layout(int dim, int n, int nslots) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     ChunkLayout L;
     L.list = 0;
-    L.count = al((size_t)n * sizeof(int));
+    L.cost = al((size_t)n * sizeof(int));
+    L.count = L.cost + al((size_t)n * sizeof(int));
     L.parts = L.count + al((size_t)(1 + nslots) * sizeof(int));  // count, then arrive[nslots]
     L.parts_e = L.parts + al((size_t)nslots * 3 * dim * dim * sizeof(dd));
     L.parts_fail = L.parts_e + al((size_t)nslots * 3 * sizeof(int));
@@ -671,7 +799,8 @@ static ChunkLayout chunk_layout(int dim, int n, int nslots) {
     return L;
 }
 
-// Survivor list and counter, arrival counters and the parts' products.
+// Survivor list with the survivors' costs and counter, arrival counters
+// and the parts' products.
 size_t chunk_scratch_bytes(int dim, int n) { return chunk_layout(dim, n, chunk_slots()).total; }
 
 template <class A>
@@ -685,6 +814,7 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     ChunkArgs C;
     C.w = W;
     C.list = (int *)(p + lay.list);
+    C.cost = (int *)(p + lay.cost);
     C.count = (int *)(p + lay.count);
     C.arrive = C.count + 1;
     C.parts = p + lay.parts;

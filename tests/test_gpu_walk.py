@@ -298,17 +298,17 @@ def test_df64_compat_matches_oracle(cuda):
 @pytest.mark.parametrize("variant,rtol", [("f64", 1e-11), ("df64", 1e-9)])
 def test_chunk_parts_agree(cuda, variant, rtol):
     """The chunked walk spreads each survivor over as many CTAs as the batch
-    leaves room for (1 to 8 parts, combined by the last part to finish) and
-    cuts runs inside lattice steps; every batch size gives a different
-    association of the same product. Zeta-start limit walks are well
-    conditioned, so every batch size -- every part count -- must give the
-    oracle's limit, p and q to rtol."""
+    leaves room for (1 to 16 parts, combined by the last part to finish,
+    more for costlier walks) and cuts runs inside lattice steps; every batch
+    size gives a different association of the same product. Zeta-start
+    limit walks are well conditioned, so every batch size -- every part
+    count -- must give the oracle's limit, p and q to rtol."""
     for p, q in [(6, 5), (3, 2), (8, 7)]:
         recs = oracle.make_inputs(p, q, 200, 0, True)
         desc = cmfw.make_desc(p, q, 1.0)
         o = oracle.walk("f64", p, q, 1.0, 1000, 50, recs, fused=True)
         assert (o["valid"] == 1).all()
-        for n in (1, 3, 20, 40, 60, 200):  # 8, 8, 7, 3, 2 and 1 parts on 148 SMs
+        for n in (1, 3, 20, 40, 60, 200):  # 16, 16, 7, 3, 2 and 1 parts on 148 SMs
             g = cmfw.walk(variant, desc, recs[:n], 1000, 50)
             np.testing.assert_array_equal(g["valid"], o["valid"][:n])
             for k in ("limit", "p", "q"):
