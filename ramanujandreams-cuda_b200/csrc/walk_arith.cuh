@@ -42,6 +42,14 @@ struct ArithF64 {
         return __fma_rn(__fma_rn(-q, s, a), inv, q);
     }
     __device__ static __forceinline__ T neg(T a) { return -a; }
+    // sum_k a[k sa] b[k sb]: the FMA chain in k order
+    template <int N>
+    __device__ static __forceinline__ T dot(const T *a, int sa, const T *b, int sb) {
+        T x = a[0] * b[0];
+#pragma unroll
+        for (int k = 1; k < N; ++k) x = __fma_rn(a[k * sa], b[k * sb], x);
+        return x;
+    }
     __device__ static __forceinline__ int hexp(T a) { return __double2hiint(a) & 0x7ff00000; }
     __device__ static __forceinline__ T scale(T a, int be) {
         return a * __hiloint2double((1023 - be) << 20, 0);
@@ -123,6 +131,39 @@ struct ArithDD {
         out.hi = __dadd_rn(q1, q2);
         out.lo = __dsub_rn(q2, __dsub_rn(out.hi, q1));
         return out;
+    }
+    // sum_k a[k sa] b[k sb], compensated: each term's exact high product
+    // and its error terms (the FMA two-product plus the cross terms) are
+    // formed independently, the high parts are summed by a pairwise tree of
+    // error-free two-sums whose errors join the terms' errors, and the pair
+    // is renormalised once. About the work of the FMA chain, at a third of
+    // its dependent depth.
+    template <int N>
+    __device__ static __forceinline__ T dot(const T *a, int sa, const T *b, int sb) {
+        double p[N], e[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const T x = a[k * sa], y = b[k * sb];
+            p[k] = __dmul_rn(x.hi, y.hi);
+            double ek = __fma_rn(x.hi, y.hi, -p[k]);
+            ek = __fma_rn(x.hi, y.lo, ek);
+            e[k] = __fma_rn(x.lo, y.hi, ek);
+        }
+#pragma unroll
+        for (int st = 1; st < N; st <<= 1) {
+#pragma unroll
+            for (int k = 0; k + st < N; k += 2 * st) {
+                const double s = __dadd_rn(p[k], p[k + st]);
+                const double bb = __dsub_rn(s, p[k]);
+                const double err = __dadd_rn(__dsub_rn(p[k], __dsub_rn(s, bb)), __dsub_rn(p[k + st], bb));
+                p[k] = s;
+                e[k] = __dadd_rn(__dadd_rn(e[k], e[k + st]), err);
+            }
+        }
+        T r;
+        r.hi = __dadd_rn(p[0], e[0]);
+        r.lo = __dsub_rn(e[0], __dsub_rn(r.hi, p[0]));
+        return r;
     }
     __device__ static __forceinline__ T neg(T a) { return T{-a.hi, -a.lo}; }
     __device__ static __forceinline__ int hexp(T a) { return __double2hiint(a.hi) & 0x7ff00000; }

@@ -151,9 +151,7 @@ __device__ __forceinline__ void par_products(const ProdTask<CA> *tasks, int ntas
             if (w < nw) {
                 const ProdTask<CA> &T = tasks[w / DD];
                 const int e = w % DD, i = e / DIM, j = e % DIM;
-                x[u] = CA::mul(T.a[i * DIM], T.b[j]);
-#pragma unroll
-                for (int k = 1; k < DIM; ++k) x[u] = CA::fma(T.a[i * DIM + k], T.b[k * DIM + j], x[u]);
+                x[u] = CA::template dot<DIM>(T.a + i * DIM, 1, T.b + j, DIM);
             }
         }
 #pragma unroll
@@ -208,10 +206,12 @@ __host__ __device__ constexpr size_t chunk_smem_bytes(int dim) {
 // 2 st m times slot a + st (for a + st inside the group), enumerated in
 // closed form. Every product's entries take whole warps (DD entries padded
 // to EW = 32 or 64 lanes), each thread ILP entries in flight; a warp's
-// largest exponent is one reduction, and the products are written back
-// rescaled into slot a once every entry is staged. Two barriers a level,
-// no atomics. wmax holds 2 ints per product. (Out of line: its registers
-// are then not counted against the walk state's.)
+// largest exponent is one reduction. Up to rank 5 (one warp per product)
+// each warp writes its product back rescaled at once: one barrier a level.
+// Above, the entries are staged and written back once both warps' maxima
+// are in: two barriers a level. No atomics. wmax holds 2 ints per product.
+// (Out of line: its registers are then not counted against the walk
+// state's.)
 __device__ __forceinline__ int level_tasks(int cnt, int st) { return cnt > st ? (cnt - st - 1) / (2 * st) + 1 : 0; }
 
 template <int DIM, class CA, int NT>
@@ -241,9 +241,7 @@ __device__ __noinline__ void group_products(typename CA::T *slots, int *sexp, co
                     const int a = tau < n0 ? g0 + 2 * st * tau
                                            : (tau < n0 + n1 ? g1 + 2 * st * (tau - n0) : g2 + 2 * st * (tau - n0 - n1));
                     const CT *A = slots + a * DD, *B = slots + (a + st) * DD;
-                    x[u] = CA::mul(A[i * DIM], B[j]);
-#pragma unroll
-                    for (int k = 1; k < DIM; ++k) x[u] = CA::fma(A[i * DIM + k], B[k * DIM + j], x[u]);
+                    x[u] = CA::template dot<DIM>(A + i * DIM, 1, B + j, DIM);
                 }
             }
 #pragma unroll
@@ -253,23 +251,38 @@ __device__ __noinline__ void group_products(typename CA::T *slots, int *sexp, co
                     const int tau = w / EW, e = w % EW;
                     const unsigned hx = e < DD ? (unsigned)CA::hexp(x[u]) : 0u;
                     const unsigned hm = __reduce_max_sync(0xffffffffu, hx);
-                    if (lane == 0) wmax[2 * tau + e / 32] = (int)hm;
-                    if (e < DD) stage[tau * DD + e] = x[u];
+                    if constexpr (EW == 32) {
+                        // one warp holds the whole product: every lane has
+                        // read its operands before the reduction, and no
+                        // other product of this level reads slot a, so the
+                        // result goes straight back into slot a
+                        const int a = tau < n0 ? g0 + 2 * st * tau
+                                               : (tau < n0 + n1 ? g1 + 2 * st * (tau - n0)
+                                                                : g2 + 2 * st * (tau - n0 - n1));
+                        const int be = (hm != 0 && hm < 0x7ff00000u) ? (int)(hm >> 20) - 1023 : 0;
+                        if (e < DD) slots[a * DD + e] = CA::scale(x[u], be);
+                        if (e == 0) sexp[a] = sexp[a] + sexp[a + st] + be;
+                    } else {
+                        if (lane == 0) wmax[2 * tau + e / 32] = (int)hm;
+                        if (e < DD) stage[tau * DD + e] = x[u];
+                    }
                 }
             }
         }
         __syncthreads();
+        if constexpr (EW > 32) {
 #pragma unroll 1
-        for (int w = tid; w < nt * DD; w += NT) {
-            const int tau = w / DD, e = w % DD;
-            const int a = tau < n0 ? g0 + 2 * st * tau
-                                   : (tau < n0 + n1 ? g1 + 2 * st * (tau - n0) : g2 + 2 * st * (tau - n0 - n1));
-            const int hm = EW > 32 ? max(wmax[2 * tau], wmax[2 * tau + 1]) : wmax[2 * tau];
-            const int be = (hm != 0 && hm < 0x7ff00000) ? (hm >> 20) - 1023 : 0;
-            slots[a * DD + e] = CA::scale(stage[w], be);
-            if (e == 0) sexp[a] = sexp[a] + sexp[a + st] + be;
+            for (int w = tid; w < nt * DD; w += NT) {
+                const int tau = w / DD, e = w % DD;
+                const int a = tau < n0 ? g0 + 2 * st * tau
+                                       : (tau < n0 + n1 ? g1 + 2 * st * (tau - n0) : g2 + 2 * st * (tau - n0 - n1));
+                const int hm = max(wmax[2 * tau], wmax[2 * tau + 1]);
+                const int be = (hm != 0 && hm < 0x7ff00000) ? (hm >> 20) - 1023 : 0;
+                slots[a * DD + e] = CA::scale(stage[w], be);
+                if (e == 0) sexp[a] = sexp[a] + sexp[a + st] + be;
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
@@ -440,6 +453,10 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
     double *s_pos = (double *)ureg;             // during the runs: [NAX][NT] positions
     CT *stage = (CT *)ureg;                     // afterwards: product staging
     __shared__ int s_ok, s_last;
+    // snapshot reduction: largest |entry| bits and a non-zero flag per
+    // snapshot, and the limit selection
+    __shared__ unsigned long long s_g[3];
+    __shared__ int s_nz[3], s_kany, s_kait, s_npush, s_nbefore;
     __shared__ double s_ls[3];
     // earliest failing axis step of this CTA's runs (fail_key), and of the
     // trajectory once the parts are combined
@@ -574,7 +591,6 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
 #pragma unroll
             for (int j = 0; j < DIM; ++j) m[r][j] = A::from((r * G + tid % G == j) ? 1.0 : 0.0);
         }
-        __syncthreads();
         {
             // this thread's run: piece i of block B
             const int NB = RT / s_c, v = tid / G;
@@ -698,51 +714,103 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
                 par_products<DIM, CA, NT>(tasks, 1, pmax, stage);
             }
             // the snapshots in the reference's form, in shared memory (the
-            // staging area is free once the products are done)
+            // staging area is free once the products are done). The rows of
+            // a snapshot share its exponent xe[k], so the reference's
+            // normalisation (normalise_rows) is a division by the largest
+            // |entry| g_k and log_scale_k = xe[k] ln 2 + log g_k; the largest
+            // entry is gathered on the bit patterns (non-negative doubles
+            // order like their bits).
             double *snap = (double *)stage;
             int *snap_e = (int *)(snap + 3 * DD);
+            if (tid < 3) {
+                s_g[tid] = 0ull;
+                s_nz[tid] = 0;
+            }
+            __syncthreads();
             for (int i = tid; i < 3 * DD; i += NT) {
                 const double v = CA::to(x[i]);
                 snap[i] = v;
-                if (!isfinite(v)) atomicAnd(&s_ok, 0);
+                if (!isfinite(v)) {
+                    atomicAnd(&s_ok, 0);
+                } else if (v != 0.0) {
+                    s_nz[i / DD] = 1;
+                    atomicMax(&s_g[i / DD], (unsigned long long)__double_as_longlong(fabs(v)));
+                }
             }
             if (tid < 3 * DIM) snap_e[tid] = xe[tid / DIM];
             __syncthreads();
-            if (tid < 3) {
-                bool nz = false;
-                for (int i = 0; i < DD; ++i) nz |= snap[tid * DD + i] != 0.0;
-                if (!nz) atomicAnd(&s_ok, 0);
-            }
+            if (tid == 0 && !(s_nz[0] && s_nz[1] && s_nz[2])) s_ok = 0;  // a zero snapshot
             __syncthreads();
             if (!s_ok) {
                 if (tid == 0) write_invalid(W, t, CMFW_TRAJ_NONFINITE);
             } else {
-                if (tid < 3) s_ls[tid] = normalise_rows(snap + tid * DD, snap_e + tid * DIM, DIM, 0.0);
+                for (int i = tid; i < 3 * DD; i += NT) snap[i] *= 1.0 / __longlong_as_double((long long)s_g[i / DD]);
+                if (tid < 3) s_ls[tid] = (0.0 + (double)xe[tid] * CMFW_LN2) + log(__longlong_as_double((long long)s_g[tid]));
+                if (tid == 0) {
+                    s_kany = 0x7fffffff;
+                    s_kait = 0x7fffffff;
+                    s_npush = 0;
+                    s_nbefore = 0;
+                }
                 __syncthreads();
-                // limit candidates in parallel, then the in-order selection
+                // Limit candidates in parallel, then the selection of
+                // compute_limits' scan: the first push (the first candidate
+                // with any, its Aitken value if it has one), the first Aitken
+                // push if fewer than CMFW_MAX_LIMITS pushes precede it, and
+                // the count of pushes capped at CMFW_MAX_LIMITS, as warp
+                // reductions.
                 const int NK = n_limit_candidates(DIM);
                 int *cf = (int *)smem;  // the run products are no longer needed
                 double *cla = (double *)(smem) + NK, *clr = cla + NK;
-                for (int k = tid; k < NK; k += NT) {
-                    double LA = 0.0, LR = 0.0;
-                    cf[k] = limit_candidate(snap, snap + DD, snap + 2 * DD, DIM, k, &LA, &LR);
-                    cla[k] = LA;
-                    clr[k] = LR;
+                for (int k0 = 0; k0 < NK; k0 += NT) {
+                    const int k = k0 + tid;
+                    int f = 0;
+                    if (k < NK) {
+                        double LA = 0.0, LR = 0.0;
+                        f = limit_candidate(snap, snap + DD, snap + 2 * DD, DIM, k, &LA, &LR);
+                        cf[k] = f;
+                        cla[k] = LA;
+                        clr[k] = LR;
+                    }
+                    const int kany = __reduce_min_sync(0xffffffffu, f ? k : 0x7fffffff);
+                    const int kait = __reduce_min_sync(0xffffffffu, (f & 1) ? k : 0x7fffffff);
+                    const int np = (int)__reduce_add_sync(0xffffffffu, (unsigned)__popc(f & 3));
+                    if ((tid & 31) == 0) {
+                        atomicMin(&s_kany, kany);
+                        atomicMin(&s_kait, kait);
+                        atomicAdd(&s_npush, np);
+                    }
                 }
                 __syncthreads();
+                if (s_npush > CMFW_MAX_LIMITS && s_kait != 0x7fffffff) {
+                    // pushes before the first Aitken one (the cap can drop it)
+                    for (int k0 = 0; k0 < NK; k0 += NT) {
+                        const int k = k0 + tid;
+                        const int np = (int)__reduce_add_sync(0xffffffffu, k < s_kait ? (unsigned)__popc(cf[k] & 3) : 0u);
+                        if ((tid & 31) == 0) atomicAdd(&s_nbefore, np);
+                    }
+                    __syncthreads();
+                }
                 if (tid == 0) {
-                    LimitScan scn;
-                    for (int k = 0; k < NK; ++k)
-                        if (cf[k]) scn.add(cf[k], cla[k], clr[k], k, DIM);
+                    const bool have_aitken = s_kait != 0x7fffffff && s_nbefore < CMFW_MAX_LIMITS;
                     cmfw_traj_out o;
                     o.valid = 1;
-                    o.n_limits = scn.n;
-                    o.limit = scn.have_aitken ? scn.first_aitken : (scn.n > 0 ? scn.first_any : (double)NAN);
+                    o.n_limits = min(s_npush, CMFW_MAX_LIMITS);
+                    int src = -1;
+                    if (have_aitken) {
+                        o.limit = cla[s_kait];
+                        src = limit_source(s_kait, DIM, true);
+                    } else if (s_npush > 0) {
+                        const bool a1 = cf[s_kany] & 1;
+                        o.limit = a1 ? cla[s_kany] : clr[s_kany];
+                        src = limit_source(s_kany, DIM, a1);
+                    } else {
+                        o.limit = (double)NAN;
+                    }
                     reduce_tail(snap, DIM, s_ls, o.limit, o);
                     W.out[t] = o;
                     if (W.status) W.status[t] = CMFW_TRAJ_OK;
-                    if (W.limit_src)
-                        W.limit_src[t] = scn.have_aitken ? scn.src_aitken : (scn.n > 0 ? scn.src_any : -1);
+                    if (W.limit_src) W.limit_src[t] = src;
                 }
             }
         }
