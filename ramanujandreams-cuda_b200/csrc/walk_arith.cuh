@@ -43,6 +43,14 @@ struct ArithF64 {
     }
     __device__ static __forceinline__ T neg(T a) { return -a; }
     // sum_k a[k sa] b[k sb]: the FMA chain in k order
+    // sum_k a[k] s[k] for FP64 scalars s (the step matrix's column)
+    template <int N>
+    __device__ static __forceinline__ T dot_s(const T *a, const double *sc) {
+        T x = a[0] * sc[0];
+#pragma unroll
+        for (int k = 1; k < N; ++k) x = __fma_rn(a[k], sc[k], x);
+        return x;
+    }
     template <int N>
     __device__ static __forceinline__ T dot(const T *a, int sa, const T *b, int sb) {
         T x = a[0] * b[0];
@@ -138,17 +146,21 @@ struct ArithDD {
     // error-free two-sums whose errors join the terms' errors, and the pair
     // is renormalised once. About the work of the FMA chain, at a third of
     // its dependent depth.
+    // sum_k a[k] s[k] for FP64 scalars s, compensated as dot() below
     template <int N>
-    __device__ static __forceinline__ T dot(const T *a, int sa, const T *b, int sb) {
+    __device__ static __forceinline__ T dot_s(const T *a, const double *sc) {
         double p[N], e[N];
 #pragma unroll
         for (int k = 0; k < N; ++k) {
-            const T x = a[k * sa], y = b[k * sb];
-            p[k] = __dmul_rn(x.hi, y.hi);
-            double ek = __fma_rn(x.hi, y.hi, -p[k]);
-            ek = __fma_rn(x.hi, y.lo, ek);
-            e[k] = __fma_rn(x.lo, y.hi, ek);
+            p[k] = __dmul_rn(a[k].hi, sc[k]);
+            e[k] = __fma_rn(a[k].lo, sc[k], __fma_rn(a[k].hi, sc[k], -p[k]));
         }
+        return sum_pairs<N>(p, e);
+    }
+    // renormalised sum of N (high, error) pairs: a pairwise tree of
+    // error-free two-sums over the high parts, the errors summed alongside
+    template <int N>
+    __device__ static __forceinline__ T sum_pairs(double (&p)[N], double (&e)[N]) {
 #pragma unroll
         for (int st = 1; st < N; st <<= 1) {
 #pragma unroll
@@ -164,6 +176,19 @@ struct ArithDD {
         r.hi = __dadd_rn(p[0], e[0]);
         r.lo = __dsub_rn(e[0], __dsub_rn(r.hi, p[0]));
         return r;
+    }
+    template <int N>
+    __device__ static __forceinline__ T dot(const T *a, int sa, const T *b, int sb) {
+        double p[N], e[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const T x = a[k * sa], y = b[k * sb];
+            p[k] = __dmul_rn(x.hi, y.hi);
+            double ek = __fma_rn(x.hi, y.hi, -p[k]);
+            ek = __fma_rn(x.hi, y.lo, ek);
+            e[k] = __fma_rn(x.lo, y.hi, ek);
+        }
+        return sum_pairs<N>(p, e);
     }
     __device__ static __forceinline__ T neg(T a) { return T{-a.hi, -a.lo}; }
     __device__ static __forceinline__ int hexp(T a) { return __double2hiint(a.hi) & 0x7ff00000; }
@@ -210,6 +235,14 @@ struct ArithFF {
     }
     // an FP64 scalar enters as its float-float rounding
     __device__ static __forceinline__ T fma_s(T a, double s, T c) { return fma(a, ff_from(s), c); }
+    // sum_k a[k] s[k] for FP64 scalars s: the chain in k order
+    template <int N>
+    __device__ static __forceinline__ T dot_s(const T *a, const double *sc) {
+        T x = mul_s(a[0], sc[0]);
+#pragma unroll
+        for (int k = 1; k < N; ++k) x = fma_s(a[k], sc[k], x);
+        return x;
+    }
     __device__ static __forceinline__ T mul_s(T a, double s) { return mul(a, ff_from(s)); }
     __device__ static __forceinline__ T div_s(T a, double s, double inv) {
         (void)s;
@@ -404,9 +437,7 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[R][DIM], int (&ex)[R
         // out[j] = m[j] + m[j+1]/a, last += (m . col)/a
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            T dot = A::mul_s(m[r][0], S.col[0]);
-#pragma unroll
-            for (int k = 1; k < DIM; ++k) dot = A::fma_s(m[r][k], S.col[k], dot);
+            const T dot = A::template dot_s<DIM>(m[r], S.col);
 #pragma unroll
             for (int j = 0; j < DIM - 1; ++j) m[r][j] = A::fma_s(m[r][j + 1], inva, m[r][j]);
             m[r][DIM - 1] = A::fma_s(dot, inva, m[r][DIM - 1]);
@@ -421,9 +452,7 @@ __device__ __forceinline__ int axis_step(typename A::T (&m)[R][DIM], int (&ex)[R
             al[DIM - 2] = m[r][DIM - 2];
 #pragma unroll
             for (int j = DIM - 3; j >= 0; --j) al[j] = A::fma_s(al[j + 1], ninva, m[r][j]);
-            T da = A::mul_s(al[0], S.col[0]);
-#pragma unroll
-            for (int k = 1; k < DIM - 1; ++k) da = A::fma_s(al[k], S.col[k], da);
+            const T da = A::template dot_s<DIM - 1>(al, S.col);
             const T tt = A::div_s(A::fma_s(da, ninva, m[r][DIM - 1]), S.sd, isd);
             // beta_j = (-1/a)^(DIM-1-j), formed as in step_matrix
             double bj = 1.0;
