@@ -242,15 +242,20 @@ typedef struct {
                        and walk only the survivors */
 } cmfw_mixed_tuning;
 size_t cmfw_mixed_workspace_bytes(int n_traj, int n_descs);
-/* tuning NULL = persistent, 128 threads, grab 32, full occupancy, no prescan. */
+/* tuning NULL = persistent, 128 threads, grab 32, full occupancy, no prescan.
+ * After the sort (on `stream`), every descriptor's walk runs on a stream of
+ * its own forked from `stream` and joined back into it, so the descriptors'
+ * walks overlap (a walk ends with its longest trajectories on a few SMs). */
 cmfw_status cmfw_walk_mixed(const cmfw_desc *descs, int n_descs, const cmfw_traj_in *d_in,
                             const cmfw_mixed_item *d_items, cmfw_traj_out *d_out, int n_traj, int h,
                             int variant, const cmfw_mixed_tuning *tuning, const cmfw_launch *launch,
                             void *stream);
 /* Autotuner: per descriptor, times every (block 64/128/256) x (grab 0/32/64)
  * on a strided sample of up to `sample` (0 = 65536) of that descriptor's
- * cost-sorted trajectories and keeps the fastest. Synchronises the stream;
- * writes scratch results into d_out. */
+ * cost-sorted trajectories; then, since the descriptors' walks run side by
+ * side, times whole tunings on the joint sample (the plain grid everywhere,
+ * the per-descriptor choices, each tile for every descriptor) and returns
+ * the fastest. Synchronises the stream; writes scratch results into d_out. */
 cmfw_status cmfw_mixed_autotune(const cmfw_desc *descs, int n_descs, const cmfw_traj_in *d_in,
                                 const cmfw_mixed_item *d_items, cmfw_traj_out *d_out, int n_traj, int h,
                                 int variant, const cmfw_launch *launch, int sample, cmfw_mixed_tuning *out,

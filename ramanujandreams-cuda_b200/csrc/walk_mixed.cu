@@ -353,34 +353,94 @@ static MixedArgs make_args(const cmfw_desc *descs, int n_descs, const cmfw_traj_
     return M;
 }
 
-// Per family: the singularity scan (persistent, cost-sorted queue), then the
-// walk of its survivors only (tuning->prescan), or the walk of every
-// trajectory.
-static cudaError_t enqueue_mixed(const MixedArgs &M, const MixedLayout &L, int variant,
-                                 const cmfw_mixed_tuning &tune, cudaStream_t s) {
-    cudaError_t e = enqueue_sort(M, L, s);
-    const bool prescan = tune.persistent && tune.prescan;
-    for (int f = 0; f < M.n_descs && e == cudaSuccess; ++f) {
-        if (!prescan) {
-            e = enqueue_family(M, f, variant, tune.tile[f], tune.persistent, s);
-            continue;
+// One family on stream s: the singularity scan (persistent, cost-sorted
+// queue) and the walk of its survivors only (prescan), or the walk of
+// every trajectory.
+static cudaError_t enqueue_family_scan_walk(const MixedArgs &M, const MixedLayout &L, int f, int variant,
+                                            const cmfw_mixed_tuning &tune, bool prescan, cudaStream_t s) {
+    if (!prescan) return enqueue_family(M, f, variant, tune.tile[f], tune.persistent, s);
+    scan_kernel_t k = pick_scan(M.descs[f].p, M.descs[f].q, M.descs[f].rank);
+    if (!k) return cudaErrorInvalidValue;
+    MixedArgs Ms = M;
+    Ms.next = L.next2;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)k, 256, 0) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        nb = 1;
+    }
+    k<<<sm_count() * nb, 256, 0, s>>>(Ms, f);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    MixedArgs Mw = M;
+    Mw.order = L.alive;
+    Mw.seg_len = L.alive_count;
+    return enqueue_family(Mw, f, variant, tune.tile[f], 1, s);
+}
+
+// Streams and events on which the families' walks run side by side: a
+// family's walk ends with its longest trajectories on a few SMs, and the
+// other families' CTAs fill the rest. One set per host thread and device,
+// kept for the process (the enqueue is also captured into graphs, where
+// the fork and join become parallel branches).
+struct ForkStreams {
+    cudaStream_t s[CMFW_MAX_MIXED_DESCS] = {};
+    cudaEvent_t start = nullptr, done[CMFW_MAX_MIXED_DESCS] = {};
+    bool ready = false;
+};
+static thread_local ForkStreams t_fork[16];
+
+static cudaError_t fork_streams(ForkStreams **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 16) return cudaErrorInvalidDevice;
+    ForkStreams &F = t_fork[dev];
+    if (!F.ready) {
+        e = cudaEventCreateWithFlags(&F.start, cudaEventDisableTiming);
+        for (int i = 0; i < CMFW_MAX_MIXED_DESCS && e == cudaSuccess; ++i) {
+            e = cudaStreamCreateWithFlags(&F.s[i], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&F.done[i], cudaEventDisableTiming);
         }
-        scan_kernel_t k = pick_scan(M.descs[f].p, M.descs[f].q, M.descs[f].rank);
-        if (!k) return cudaErrorInvalidValue;
-        MixedArgs Ms = M;
-        Ms.next = L.next2;
-        int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)k, 256, 0) != cudaSuccess || nb < 1)
-            nb = 1;
-        k<<<sm_count() * nb, 256, 0, s>>>(Ms, f);
-        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        F.ready = true;
+    }
+    *out = &F;
+    return cudaSuccess;
+}
+
+// Per family, on its own stream forked from s and joined back into s: the
+// singularity scan (persistent, cost-sorted queue) and the walk of its
+// survivors only (tuning->prescan), or the walk of every trajectory. The
+// sort comes first, on s (enqueue_mixed).
+static cudaError_t enqueue_families_forked(const MixedArgs &M, const MixedLayout &L, int variant,
+                                           const cmfw_mixed_tuning &tune, cudaStream_t s) {
+    ForkStreams *F = nullptr;
+    cudaError_t e = fork_streams(&F);
+    if (e == cudaSuccess) e = cudaEventRecord(F->start, s);
+    const bool prescan = tune.persistent && tune.prescan;
+    int forked = 0;
+    for (int f = 0; f < M.n_descs && e == cudaSuccess; ++f) {
+        cudaStream_t fs = F->s[f];
+        e = cudaStreamWaitEvent(fs, F->start, 0);
         if (e != cudaSuccess) break;
-        MixedArgs Mw = M;
-        Mw.order = L.alive;
-        Mw.seg_len = L.alive_count;
-        e = enqueue_family(Mw, f, variant, tune.tile[f], 1, s);
+        forked = f + 1;
+        e = enqueue_family_scan_walk(M, L, f, variant, tune, prescan, fs);
+        const cudaError_t r = cudaEventRecord(F->done[f], fs);  // also after an error: the join needs it
+        if (e == cudaSuccess) e = r;
+    }
+    // join every forked stream back, also after an error (a capture must
+    // end with its branches joined)
+    for (int f = 0; f < forked; ++f) {
+        const cudaError_t j = cudaStreamWaitEvent(s, F->done[f], 0);
+        if (e == cudaSuccess) e = j;
     }
     return e;
+}
+
+static cudaError_t enqueue_mixed(const MixedArgs &M, const MixedLayout &L, int variant,
+                                 const cmfw_mixed_tuning &tune, cudaStream_t s) {
+    const cudaError_t e = enqueue_sort(M, L, s);
+    return e != cudaSuccess ? e : enqueue_families_forked(M, L, variant, tune, s);
 }
 
 }  // namespace cmfw
@@ -505,8 +565,58 @@ cmfw_status cmfw_mixed_autotune(const cmfw_desc *descs, int n_descs, const cmfw_
                 }
             }
     }
+    // The families walk side by side (enqueue_mixed), so the per-family
+    // times do not add up: compare whole-batch tile sets on a joint sample
+    // (every family's strided sample) -- the plain grid, the per-family
+    // choices, and each tile for every family -- and keep the fastest.
+    std::vector<int> so_all, sb_all(CMFW_MAX_MIXED_DESCS + 1, 0);
+    for (int f = 0; f < n_descs; ++f) {
+        const int len = begin[f + 1] - begin[f];
+        const int m = len <= 0 ? 0 : (len < sample ? len : sample);
+        for (int i = 0; i < m; ++i) so_all.push_back(order[begin[f] + (int)(((long long)i * len) / m)]);
+        sb_all[f + 1] = (int)so_all.size();
+    }
+    for (int g = n_descs + 1; g <= CMFW_MAX_MIXED_DESCS; ++g) sb_all[g] = (int)so_all.size();
+    int *d_jorder = nullptr;
+    if (e == cudaSuccess && !so_all.empty()) {
+        e = cudaMalloc(&d_jorder, sizeof(int) * so_all.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_jorder, so_all.data(), sizeof(int) * so_all.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(d_sbegin, sb_all.data(), sizeof(int) * sb_all.size(), cudaMemcpyHostToDevice);
+        MixedArgs Mj = M;
+        Mj.order = d_jorder;
+        Mj.begin = d_sbegin;
+        Mj.next = d_snext;
+        const cmfw_mixed_tuning per_family = *out;
+        float best = 1e30f;
+        for (int c = -2; c < 9 && e == cudaSuccess; ++c) {
+            cmfw_mixed_tuning t = per_family;
+            if (c == -2) t.persistent = 0;  // the plain 256-thread grid everywhere
+            if (c >= 0)
+                for (int f = 0; f < n_descs; ++f) {
+                    t.tile[f].block_size = blocks[c / 3];
+                    t.tile[f].grab = grabs[c % 3];
+                    t.tile[f].ctas_per_sm = 0;
+                }
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {  // warm-up, then timed
+                e = cudaMemsetAsync(d_snext, 0, sizeof(int) * CMFW_MAX_MIXED_DESCS, s);
+                if (e == cudaSuccess) e = cudaEventRecord(a, s);
+                if (e == cudaSuccess) e = enqueue_families_forked(Mj, L, variant, t, s);
+                if (e == cudaSuccess) e = cudaEventRecord(b, s);
+                if (e == cudaSuccess) e = cudaEventSynchronize(b);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+            }
+            if (e == cudaSuccess && ms < best) {
+                best = ms;
+                *out = t;
+            }
+        }
+    }
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
+    cudaFree(d_jorder);
     cudaFree(d_sorder);
     cudaFree(d_sbegin);
     cudaFree(d_snext);
