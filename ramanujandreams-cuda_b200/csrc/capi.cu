@@ -97,19 +97,27 @@ cmfw_status ensure_compat_table() {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Device copies of cmfw_walk_host's records, one pair per calling thread
-// and device, kept between calls (the call synchronises before returning).
+// Device copies of cmfw_walk_host's records and its timing events, one set
+// per calling thread and device, kept between calls (the call synchronises
+// before returning).
 struct Staging {
     void *in = nullptr, *out = nullptr;
     int cap = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // the call's timing events
 };
 thread_local std::map<int, Staging> t_staging;
 
-cudaError_t host_staging(int n, cmfw_traj_in **in, cmfw_traj_out **out) {
+cudaError_t host_staging(int n, cmfw_traj_in **in, cmfw_traj_out **out, cudaEvent_t **ev) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     Staging &s = t_staging[dev];
+    for (int i = 0; i < 4; ++i)
+        if (!s.ev[i]) {
+            e = cudaEventCreate(&s.ev[i]);
+            if (e != cudaSuccess) return e;
+        }
+    *ev = s.ev;
     if (s.cap < n) {
         cudaFree(s.in);
         cudaFree(s.out);
@@ -405,9 +413,8 @@ cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cm
     }
     cmfw_traj_in *d_in = nullptr;
     cmfw_traj_out *d_out = nullptr;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaError_t e = host_staging(n, &d_in, &d_out);
-    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ev[i]);
+    cudaEvent_t *ev = nullptr;
+    cudaError_t e = host_staging(n, &d_in, &d_out, &ev);
     if (e != cudaSuccess) {
         st = set_err(CMFW_ENOMEM, "device buffers for %d trajectories: %s", n, cudaGetErrorString(e));
     } else {
@@ -436,8 +443,6 @@ cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cm
             if (total_ms) *total_ms = b;
         }
     }
-    for (int i = 0; i < 4; ++i)
-        if (ev[i]) cudaEventDestroy(ev[i]);
     return st;
 }
 

@@ -51,6 +51,8 @@
 // instructions, no such guarantee); df64 runs in float-float with FP64
 // products (ArithFF).
 #include <algorithm>
+#include <mutex>
+#include <vector>
 
 #include "walk_arith.cuh"
 
@@ -75,6 +77,9 @@ constexpr int kFilterThreads = 64;
 
 template <int P_, int Q_, int DIM>
 __global__ void __launch_bounds__(kFilterThreads) walk_prefix_kernel(ChunkArgs C) {
+    // the chunk kernel may be scheduled now: it waits for this grid's end
+    // (cudaGridDependencySynchronize) before it reads anything written here
+    cudaTriggerProgrammaticLaunchCompletion();
     const WalkArgs &W = C.w;
     constexpr int NAX = (P_ > 0) ? (P_ + Q_) : CMFW_MAX_AXES;
     constexpr int PM = (P_ > 0) ? P_ : 8;
@@ -483,6 +488,10 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
     // CTAs stride over the list. Warp 0 finds this CTA's part; the values
     // are kept in shared memory, like the run geometry below.
     __shared__ int s_count, s_bal, s_b0, s_part0, s_np0, s_first0;
+    // The filter kernel is launched before this one with programmatic
+    // stream serialisation: wait (in hardware) until it has finished and
+    // its survivor list is visible. Nothing above reads its outputs.
+    cudaGridDependencySynchronize();
     if (tid < 32) {
         const int count = *C.count;
         const int Gr = min((int)gridDim.x, C.nslots);
@@ -842,14 +851,61 @@ static ChunkPick<A> pick_chunk(int p, int q, int dim) {
     return ChunkPick<A>{nullptr, nullptr, 0};
 }
 
+// SMs of the current device, and per chunk kernel its dynamic shared
+// memory attribute and CTAs per SM: queried once per device (a walk is
+// ~0.1 ms, and each query is a runtime call on its host path).
+static int device_sms() {
+    static std::mutex mu;
+    static int sms_of[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 148;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (sms_of[dev] == 0) {
+        int sms = 148;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            sms = 148;
+        }
+        sms_of[dev] = sms;
+    }
+    return sms_of[dev];
+}
+
+struct ChunkKernelInfo {
+    const void *fn;
+    int dev, per_sm;
+};
+
+static cudaError_t chunk_kernel_setup(const void *fn, int threads, size_t shmem, int *per_sm) {
+    static std::mutex mu;
+    static std::vector<ChunkKernelInfo> known;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    for (const ChunkKernelInfo &k : known)
+        if (k.fn == fn && k.dev == dev) {
+            *per_sm = k.per_sm;
+            return cudaSuccess;
+        }
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+    if (e != cudaSuccess) return e;
+    int n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, shmem) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        n = 1;
+    }
+    known.push_back(ChunkKernelInfo{fn, dev, n});
+    *per_sm = n;
+    return cudaSuccess;
+}
+
 // Product slots for trajectories walked in parts: one per CTA of the
 // chunk grid, which is never larger.
-static int chunk_slots() {
-    int dev = 0, sms = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaGetLastError();
-    return 2 * sms;
-}
+static int chunk_slots() { return 2 * device_sms(); }
 
 struct ChunkLayout {
     size_t list, cost, count, parts, parts_e, parts_fail, total;
@@ -892,8 +948,8 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     C.prefix_steps = prefix_steps;
     const int NT = chunk_threads(dim);
     const size_t shmem = chunk_smem_bytes<typename A::Combine::T>(dim);
-    cudaError_t e = cudaFuncSetAttribute((const void *)k.chunk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)shmem);
+    int per_sm = 1;
+    cudaError_t e = chunk_kernel_setup((const void *)k.chunk, NT, shmem, &per_sm);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(C.count, 0, (size_t)(1 + nslots) * sizeof(int), s);
     if (e != cudaSuccess) return e;
@@ -902,18 +958,24 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     if (e != cudaSuccess) return e;
     // persistent grid: as many CTAs as can be resident at once, at most
     // kMaxParts per trajectory and one per product slot
-    int dev = 0, sms = 148, per_sm = 1;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k.chunk, NT, shmem) != cudaSuccess ||
-        per_sm < 1) {
-        cudaGetLastError();
-        per_sm = 1;
-    }
-    long long grid = (long long)sms * per_sm;
+    long long grid = (long long)device_sms() * per_sm;
     grid = std::min<long long>(grid, (long long)std::max(n, 1) * kMaxParts);
     grid = std::min<long long>(grid, nslots);
-    k.chunk<<<(unsigned)grid, NT, shmem, s>>>(C);
-    return cudaGetLastError();
+    // launched as the filter's programmatic dependent: its CTAs may be set
+    // up while the filter drains (cudaGridDependencySynchronize in the
+    // kernel orders the reads)
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = shmem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, k.chunk, C);
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 // ff selects the df64 walk (float-float runs); otherwise the f64 walk with
