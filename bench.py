@@ -251,9 +251,13 @@ def main_cmfw(args):
                                          ctypes.c_void_p(pin_out.data_ptr()), n, N, H, 8,
                                          ctypes.byref(launch), ctypes.byref(kms), ctypes.byref(tms)))
 
-    e2e_step()
+    # host wall clock is noisier than device events: average over at least
+    # 50 calls (each a full step: copies in, walk, results out)
+    for _ in range(3):
+        e2e_step()
+    e2e_calls = max(args.steps, 50)
     e2e_ms = []
-    for k in range(args.steps):
+    for k in range(e2e_calls):
         flush.fill_(k & 0xff)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -305,7 +309,7 @@ def main_cmfw(args):
         "best_delta_per_gpu_s": (best_delta / (t_max * world)) if best_delta is not None else None,
         "gpu_launches": 2 * args.steps,  # prefix + chunk kernel per step
         "e2e": {"value": total_ver / t_e2e_max, "unit": "verified traj/s",
-                "h2d_bytes_per_step": n * 192, "d2h_bytes_per_step": n * 56},
+                "h2d_bytes_per_step": n * 192, "d2h_bytes_per_step": n * 56, "calls": e2e_calls},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
                      "frac": achieved / peak_fp64 if peak_fp64 else None,
                      "peak_source": "in-run FP64 FMA probe (cmfw_pipe_peak); MEASURED_PEAKS.json has no FP64 figure",

@@ -16,7 +16,7 @@
 namespace cmfw {
 cudaError_t launch_walk_seq(const WalkArgs &W, bool ff, int block, cudaStream_t s);
 cudaError_t launch_walk_chunked(const WalkArgs &W, bool ff, int threads, void *scratch, int prefix_steps,
-                                cudaStream_t s);
+                                cudaStream_t s, const HostGather *hg = nullptr);
 size_t chunk_scratch_bytes(int dim, int n);
 cudaError_t launch_walk_df64_compat(const WalkArgs &W, int block, cudaStream_t s);
 cudaError_t launch_walk_rns(const WalkArgs &W, int n_primes, int trace_steps, uint32_t *trace_res,
@@ -104,6 +104,14 @@ struct Staging {
     void *in = nullptr, *out = nullptr;
     int cap = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // the call's timing events
+    // chunked walks: a stream that copies the results back while the chunk
+    // kernel runs, its event, the filter's event, and the mapped pinned
+    // buffers that receive the survivors' results (cap entries)
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_done = nullptr, filter_done = nullptr;
+    int *h_count = nullptr, *h_idx = nullptr;
+    cmfw_traj_out *h_rec = nullptr;
+    int h_cap = 0;
 };
 thread_local std::map<int, Staging> t_staging;
 
@@ -130,6 +138,35 @@ cudaError_t host_staging(int n, cmfw_traj_in **in, cmfw_traj_out **out, cudaEven
     }
     *in = (cmfw_traj_in *)s.in;
     *out = (cmfw_traj_out *)s.out;
+    return cudaSuccess;
+}
+
+// The overlap machinery of cmfw_walk_host's chunked walks, for n results.
+cudaError_t host_gather(int n, Staging **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    Staging &s = t_staging[dev];
+    if (!s.side) {
+        e = cudaStreamCreateWithFlags(&s.side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.side_done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.filter_done, cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    if (s.h_cap < n) {
+        cudaFreeHost(s.h_count);
+        cudaFreeHost(s.h_idx);
+        cudaFreeHost(s.h_rec);
+        s.h_count = s.h_idx = nullptr;
+        s.h_rec = nullptr;
+        s.h_cap = 0;
+        e = cudaHostAlloc(&s.h_count, sizeof(int), cudaHostAllocMapped);
+        if (e == cudaSuccess) e = cudaHostAlloc(&s.h_idx, sizeof(int) * (size_t)n, cudaHostAllocMapped);
+        if (e == cudaSuccess) e = cudaHostAlloc(&s.h_rec, sizeof(cmfw_traj_out) * (size_t)n, cudaHostAllocMapped);
+        if (e != cudaSuccess) return e;
+        s.h_cap = n;
+    }
+    *out = &s;
     return cudaSuccess;
 }
 
@@ -399,6 +436,50 @@ void cmfw_mt64_fill_at(uint64_t seed, uint64_t offset, uint64_t *out, size_t n) 
     for (size_t i = 0; i < n; ++i) out[i] = rng();
 }
 
+// cmfw_walk_host for the chunked f64 / df64 walks, the inputs already on
+// their way to d_in: the results are copied back on a side stream as soon
+// as the filter has written every failed trajectory's record (the copy
+// overlaps the chunk kernel), and the survivors' records, which the chunk
+// kernel writes afterwards, come back through mapped pinned memory and
+// are placed over their stale copies.
+static cmfw_status walk_host_chunked(bool ff, const cmfw_desc *desc, cmfw_traj_out *h_out, cmfw_traj_in *d_in,
+                                     cmfw_traj_out *d_out, int n, int N, int h, const cmfw_launch *launch,
+                                     cudaEvent_t *ev, float *kernel_ms, float *total_ms) {
+    Staging *S = nullptr;
+    cudaError_t e = host_gather(n, &S);
+    if (e != cudaSuccess) return set_err(CMFW_ENOMEM, "host buffers for %d results: %s", n, cudaGetErrorString(e));
+    WalkArgs W;
+    cmfw_status st = prepare(desc, d_in, d_out, n, N, h, launch, 0, W);
+    if (st != CMFW_OK) return st;
+    HostGather hg;
+    hg.filter_done = S->filter_done;
+    e = cudaHostGetDevicePointer((void **)&hg.count, S->h_count, 0);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&hg.idx, S->h_idx, 0);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&hg.rec, S->h_rec, 0);
+    if (e != cudaSuccess) return cuda_err(e, "mapped result buffers");
+    e = launch_walk_chunked(W, ff, block_of(launch), chunk_scratch(W), kPrefixSteps, 0, &hg);
+    if (e != cudaSuccess) return cuda_err(e, ff ? "df64 walk launch" : "f64 walk launch");
+    cudaEventRecord(ev[2], 0);
+    e = cudaStreamWaitEvent(S->side, S->filter_done, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h_out, d_out, sizeof(cmfw_traj_out) * (size_t)n, cudaMemcpyDeviceToHost, S->side);
+    if (e == cudaSuccess) e = cudaEventRecord(S->side_done, S->side);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(0, S->side_done, 0);
+    if (e != cudaSuccess) st = cuda_err(e, "result copy");
+    cudaEventRecord(ev[3], 0);
+    e = cudaEventSynchronize(ev[3]);
+    if (e != cudaSuccess && st == CMFW_OK) st = cuda_err(e, "walk execution");
+    if (st != CMFW_OK) return st;
+    const int c = *(volatile int *)S->h_count;
+    for (int i = 0; i < c; ++i) h_out[S->h_idx[i]] = S->h_rec[i];
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, ev[1], ev[2]);
+    cudaEventElapsedTime(&b, ev[0], ev[3]);
+    if (kernel_ms) *kernel_ms = a;
+    if (total_ms) *total_ms = b;
+    return CMFW_OK;
+}
+
 cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cmfw_traj_in *h_in,
                            cmfw_traj_out *h_out, int n, int N, int h, int n_primes, const cmfw_launch *launch,
                            float *kernel_ms, float *total_ms) {
@@ -422,6 +503,13 @@ cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cm
         e = cudaMemcpyAsync(d_in, h_in, sizeof(cmfw_traj_in) * (size_t)n, cudaMemcpyHostToDevice, 0);
         if (e != cudaSuccess) st = cuda_err(e, "input copy");
         cudaEventRecord(ev[1], 0);
+        const int flags = launch ? launch->flags : 0;
+        const bool chunked = (variant == CMFW_VARIANT_F64 || variant == CMFW_VARIANT_DF64) &&
+                             !(flags & CMFW_F_SEQUENTIAL) &&
+                             !(variant == CMFW_VARIANT_DF64 && (flags & CMFW_F_DF64_COMPAT));
+        if (st == CMFW_OK && chunked)
+            return walk_host_chunked(variant == CMFW_VARIANT_DF64, desc, h_out, d_in, d_out, n, N, h, launch, ev,
+                                     kernel_ms, total_ms);
         if (st == CMFW_OK) {
             if (variant == CMFW_VARIANT_F64) st = cmfw_walk_f64(desc, d_in, d_out, n, N, h, launch, nullptr);
             else if (variant == CMFW_VARIANT_DF64) st = cmfw_walk_df64(desc, d_in, d_out, n, N, h, launch, nullptr);

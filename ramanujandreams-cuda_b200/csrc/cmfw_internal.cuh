@@ -14,6 +14,16 @@
 
 namespace cmfw {
 
+// For cmfw_walk_host's chunked walks: an event recorded between the filter
+// and the chunk kernel (every result the filter writes is final by then),
+// and host-readable buffers (mapped pinned memory, device addresses) that
+// receive the survivors' indices, records and number after the walk.
+struct HostGather {
+    cudaEvent_t filter_done;
+    int *count, *idx;
+    cmfw_traj_out *rec;
+};
+
 // Arguments common to the plain walk kernels.
 struct WalkArgs {
     const cmfw_traj_in *in;

@@ -927,8 +927,24 @@ static ChunkLayout chunk_layout(int dim, int n, int nslots) {
 // and the parts' products.
 size_t chunk_scratch_bytes(int dim, int n) { return chunk_layout(dim, n, chunk_slots()).total; }
 
+// The survivors' results of a chunked walk, gathered for the host entry
+// point: index and record of each into buffers the host reads (mapped
+// pinned memory), and their number.
+__global__ void gather_survivors_kernel(const cmfw_traj_out *out, const int *list, const int *count,
+                                        int *h_count, int *h_idx, cmfw_traj_out *h_rec) {
+    const int c = *count;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *h_count = c;
+    if (i < c) {
+        const int t = list[i];
+        h_idx[i] = t;
+        h_rec[i] = out[t];
+    }
+}
+
 template <class A>
-static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_steps, cudaStream_t s) {
+static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_steps, cudaStream_t s,
+                                  const HostGather *hg = nullptr) {
     ChunkPick<A> k = pick_chunk<A>(W.p, W.q, W.dim);
     if (!k.prefix) return cudaErrorInvalidValue;
     const int dim = W.dim, n = W.n_traj;
@@ -956,6 +972,10 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     k.prefix<<<(n + kFilterThreads - 1) / kFilterThreads, kFilterThreads, 0, s>>>(C);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (hg) {
+        e = cudaEventRecord(hg->filter_done, s);
+        if (e != cudaSuccess) return e;
+    }
     // persistent grid: as many CTAs as can be resident at once, at most
     // kMaxParts per trajectory and one per product slot
     long long grid = (long long)device_sms() * per_sm;
@@ -975,17 +995,20 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     e = cudaLaunchKernelEx(&cfg, k.chunk, C);
-    return e != cudaSuccess ? e : cudaGetLastError();
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess || !hg) return e;
+    gather_survivors_kernel<<<(n + 255) / 256, 256, 0, s>>>(W.out, C.list, C.count, hg->count, hg->idx, hg->rec);
+    return cudaGetLastError();
 }
 
 // ff selects the df64 walk (float-float runs); otherwise the f64 walk with
 // double-double runs, or plain FP64 runs with CMFW_F_PLAIN_RUNS.
 cudaError_t launch_walk_chunked(const WalkArgs &W, bool ff, int threads, void *scratch, int prefix_steps,
-                                cudaStream_t s) {
+                                cudaStream_t s, const HostGather *hg) {
     (void)threads;
-    if (ff) return launch_chunk_t<ArithFF>(W, scratch, prefix_steps, s);
-    if (W.flags & CMFW_F_PLAIN_RUNS) return launch_chunk_t<ArithF64>(W, scratch, prefix_steps, s);
-    return launch_chunk_t<ArithDD>(W, scratch, prefix_steps, s);
+    if (ff) return launch_chunk_t<ArithFF>(W, scratch, prefix_steps, s, hg);
+    if (W.flags & CMFW_F_PLAIN_RUNS) return launch_chunk_t<ArithF64>(W, scratch, prefix_steps, s, hg);
+    return launch_chunk_t<ArithDD>(W, scratch, prefix_steps, s, hg);
 }
 
 }  // namespace cmfw
