@@ -345,7 +345,13 @@ typedef enum { CMFW_VARIANT_F64 = 0, CMFW_VARIANT_DF64 = 1, CMFW_VARIANT_RNS = 2
 
 /* Copies h_in to the device, runs the variant, copies results to h_out and
  * synchronises. *kernel_ms (optional) receives the event-timed duration of
- * the walk kernels alone; *total_ms (optional) the copies included. */
+ * the walk kernels alone; *total_ms (optional) the copies included. For the
+ * chunked f64 and df64 walks the results start back to h_out on a side
+ * stream once the filter kernel has written every early failure, and the
+ * survivors' records, finished later by the chunk kernel, arrive through
+ * mapped pinned memory and overwrite their stale copies before the call
+ * returns. Device and pinned staging buffers are kept per calling thread
+ * and device between calls. */
 cmfw_status cmfw_walk_host(cmfw_variant variant, const cmfw_desc *desc, const cmfw_traj_in *h_in,
                            cmfw_traj_out *h_out, int n_traj, int N, int h, int n_primes,
                            const cmfw_launch *launch, float *kernel_ms, float *total_ms);
