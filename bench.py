@@ -16,7 +16,16 @@ walks its own seeded batch (weak scaling; no collective on the data path,
 one small gather of counters at the end).
 
 --impl reference times the reference's own kernel bodies compiled for the
-host (oracle/_ref, OpenMP over all host cores) on the same batch.
+host (oracle/_ref, OpenMP over all host cores) on the same batch and
+verifies them with the oracle alone (the estimator of each limit from the
+oracle's restatement of the reference's reduction, exact values from the
+oracle's exact walk modulo primes); it loads nothing of the product.
+
+The default line also carries the per-result error distribution
+(`accuracy`), the plain one-thread-per-trajectory kernels on the same batch
+(`plain`: this project's sequential kernel and the reference's own
+walk_kernel_f64 built for sm_100a), and the chunked walk on 2,000
+directions whose walks stay valid (`valid_directions`, with its roofline).
 """
 import argparse
 import json
@@ -49,6 +58,8 @@ def parse():
     ap.add_argument("--impl", default="cmfw", choices=["cmfw", "reference"])
     ap.add_argument("--variant", default="f64", choices=["f64", "df64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave out the plain-kernel comparison and the valid-direction workload")
     ap.add_argument("--workload", default="zeta6f5", choices=["zeta6f5", "mixed", "proposal"],
                     help="zeta6f5: the headline 6F5 delta search; mixed: the mixed-family batch "
                          "(10^6 trajectories, N log-uniform 200..5000) in one graph launch; proposal: the "
@@ -169,6 +180,44 @@ def cpu_reference(records, threads, budget_s=8.0, max_passes=20):
     return kind, out, times
 
 
+def reference_sources(records, ref_out, threads, fused=False, rtol=0.0):
+    """The estimator behind each of the reference's limits (ratio and
+    method, as cmfw's limit_src): the oracle's restatement of the
+    reference's reduction reports it. A row keeps it only where the
+    oracle's limit equals the reference's (bit for bit with rtol = 0, the
+    host builds; within rtol for the reference's GPU build, whose FMA
+    contraction rounds differently); other rows get -1 (unattributed, never
+    verified)."""
+    import oracle
+    o_out, src = oracle.walk_f64_src(P, Q, Z, N, H, records, fused=fused, threads=threads)
+    a, b = np.asarray(ref_out["limit"]), np.asarray(o_out["limit"])
+    with np.errstate(invalid="ignore"):
+        same = (a == b) | (np.isnan(a) & np.isnan(b)) | (np.abs(a - b) <= rtol * np.abs(b))
+    same &= np.asarray(ref_out["valid"]) == np.asarray(o_out["valid"])
+    return np.where(same, src, -1).astype(np.int32), int((~same).sum())
+
+
+def accuracy(rel_err, floor, valid):
+    """Per-result error against the exact value of each result's own
+    estimator: counts within 1e-13, 1e-11 and 1e-10, each beside the number
+    of results whose estimator's rounding floor (the error double-precision
+    ratios alone leave) is within the same bound, and the rows."""
+    idx = np.nonzero(valid)[0]
+    rel = np.asarray(rel_err)[idx]
+    fl = np.asarray(floor)[idx] if floor is not None else np.full(len(idx), np.nan)
+    out = {"valid": int(len(idx)), "comparable": int(np.isfinite(rel).sum()), "within": {}}
+    if floor is not None:
+        out["floor_within"] = {}
+    for b in (1e-13, 1e-11, 1e-10):
+        with np.errstate(invalid="ignore"):
+            out["within"][f"{b:.0e}"] = int((rel <= b).sum())
+            if floor is not None:
+                out["floor_within"][f"{b:.0e}"] = int((fl <= b).sum())
+    out["rows"] = [[int(t), None if not np.isfinite(r) else float(f"{r:.3e}"),
+                    None if not np.isfinite(f) else float(f"{f:.3e}")] for t, r, f in zip(idx, rel, fl)]
+    return out
+
+
 def verify_counts(desc, records, results, limit_src):
     from cmfw import exact
     v = exact.verify(desc, records, results, limit_src, N, H, rtol=RTOL)
@@ -176,6 +225,94 @@ def verify_counts(desc, records, results, limit_src):
     deltas = results["delta"][ok]
     deltas = deltas[np.isfinite(deltas)]
     return int(ok.sum()), v, (float(deltas.max()) if deltas.size else None)
+
+
+def time_events(fn, steps, flush):
+    """Mean device time (s) of fn() over `steps` calls, CUDA events on the
+    current stream, L2 flushed before each."""
+    import torch
+    ms = []
+    for k in range(steps):
+        flush.fill_(k & 0xff)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return float(np.mean(ms)) / 1e3
+
+
+def plain_kernels(desc, records, d_in, flush, steps):
+    """The one-thread-per-trajectory f64 walks on the same batch: this
+    project's sequential kernel (CMFW_F_SEQUENTIAL) and the reference's own
+    walk_kernel_f64 built unchanged for sm_100a (oracle/_ref), each with its
+    verified count -- the plain kernels the chunked walk is measured
+    against."""
+    import torch
+    import cmfw
+    import oracle
+    n = len(records)
+    out = {}
+    d_out = cmfw.out_buffer(n)
+    d_src = torch.empty(n, dtype=torch.int32, device="cuda")
+    seq = lambda: cmfw.launch_walk("f64", desc, d_in, d_out, n, N, H, flags=cmfw.F_SEQUENTIAL, d_limit_src=d_src)
+    seq()
+    torch.cuda.synchronize()
+    t = time_events(seq, steps, flush)
+    res = cmfw.records_from_device(d_out, n)
+    nv, _, _ = verify_counts(desc, records, res, d_src.cpu().numpy())
+    out["cmfw_sequential"] = {"ms_per_step": t * 1e3, "n_verified": nv, "verified_traj_per_s": nv / t,
+                              "kernel": "walk_float_kernel (one thread per trajectory)"}
+    if oracle.have_ref_gpu("f64"):
+        d_ref = torch.empty((n, 64), dtype=torch.uint8, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        ref = lambda: oracle.ref_gpu_launch("f64", P, Q, Z, N, H, d_in.data_ptr(), d_ref.data_ptr(), n,
+                                            stream=stream)
+        ref()
+        torch.cuda.synchronize()
+        t = time_events(ref, steps, flush)
+        rout = d_ref.cpu().numpy().reshape(-1).view(oracle.OUT_F64_DTYPE)
+        src, unattributed = reference_sources(records, rout, 0, fused=True, rtol=1e-9)
+        nv, _, _ = verify_counts(desc, records, rout, src)
+        out["reference_sm100a"] = {"ms_per_step": t * 1e3, "n_verified": nv, "verified_traj_per_s": nv / t,
+                                   "n_valid": int((rout["valid"] == 1).sum()), "unattributed_rows": unattributed,
+                                   "kernel": "walk_kernel_f64 (cuda/cmf_walk_f64.cu:94-154), nvcc -O3 sm_100a, "
+                                             "block 256"}
+    else:
+        out["reference_sm100a"] = {"unavailable": "oracle/_ref/libref_gpu_f64.so not built"}
+    return out
+
+
+def valid_direction_run(desc, flush, steps, n=2000):
+    """The chunked walk on non-degenerate work: n directions of the headline
+    search (seeded rejection sampling, only those whose walk stays valid),
+    same N and h; verified count and the FP64-pipe roofline there."""
+    import torch
+    import cmfw
+    import cmfw.workloads as wl
+    t0 = time.perf_counter()
+    recs = wl.valid_directions(P, Q, n, SEED, z=Z, N=N, h=H)
+    t_gen = time.perf_counter() - t0
+    d_in = cmfw.to_device(recs)
+    d_out = cmfw.out_buffer(n)
+    d_src = torch.empty(n, dtype=torch.int32, device="cuda")
+    step = lambda: cmfw.launch_walk("f64", desc, d_in, d_out, n, N, H, d_limit_src=d_src)
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    t = time_events(step, steps, flush)
+    res = cmfw.records_from_device(d_out, n)
+    valid = res["valid"] == 1
+    t0 = time.perf_counter()
+    nv, v, _ = verify_counts(desc, recs, res, d_src.cpu().numpy())
+    t_ver = time.perf_counter() - t0
+    flops = flops_per_traj(recs, valid, desc.rank)
+    return {"workload": f"{n} valid directions of the 6F5 zeta search (rejection-sampled, seed {SEED}), "
+                        "N=1000, h=50", "ms_per_step": t * 1e3, "n_valid": int(valid.sum()), "n_verified": nv,
+            "verified_traj_per_s": nv / t, "traj_per_s": n / t, "flops_per_launch": flops,
+            "achieved_tflops": flops / t / 1e12, "accuracy": accuracy(v["rel_err"], v["floor"], valid),
+            "generate_s": t_gen, "verify_s": t_ver}
 
 
 def gather_sum(x, world):
@@ -329,23 +466,45 @@ def main_cmfw(args):
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         kind, cpu_out, times = cpu_reference(records, threads)
-        cpu_ver, _, _ = verify_counts(desc, records, cpu_out, src)
+        cpu_src, _ = reference_sources(records, cpu_out, threads)
+        cpu_ver, _, _ = verify_counts(desc, records, cpu_out, cpu_src)
         t_cpu = float(np.mean(times))
         line["cpu_baseline"] = {"value": cpu_ver / t_cpu, "unit": "verified traj/s", "cores": threads,
                                 "kind": kind,
                                 "sample": f"the full batch ({n} trajectories) x {len(times)} passes, "
-                                          f"{t_cpu * 1e3:.1f} ms per pass"}
+                                          f"{t_cpu * 1e3:.1f} ms per pass",
+                                "verification": "estimator of each limit from the oracle's restatement of the "
+                                                "reference's reduction, exact values from the GPU exact walk"}
+    line["accuracy"] = accuracy(vinfo["rel_err"], vinfo["floor"], results["valid"] == 1)
+    if world == 1 and not args.no_extras:
+        plain = plain_kernels(desc, records, d_in, flush, 3)
+        ref = plain.get("reference_sm100a", {})
+        if ref.get("verified_traj_per_s"):
+            plain["chunked_vs_reference_sm100a"] = value / ref["verified_traj_per_s"]
+        if plain["cmfw_sequential"]["verified_traj_per_s"]:
+            plain["chunked_vs_cmfw_sequential"] = value / plain["cmfw_sequential"]["verified_traj_per_s"]
+        line["plain"] = plain
+        vd = valid_direction_run(desc, flush, args.steps)
+        vd["roofline"] = {"bound": "fp64", "achieved": vd["achieved_tflops"], "peak": peak_fp64, "unit": "TFLOP/s",
+                          "frac": vd["achieved_tflops"] / peak_fp64 if peak_fp64 else None}
+        line["valid_directions"] = vd
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
 
 
 def main_reference(args):
+    """The reference's own CPU path on the same batch (oracle/_ref: its
+    kernel bodies compiled for the host, OpenMP over all host cores), verified
+    by the oracle alone: the estimator of each limit from the oracle's
+    restatement of the reference's reduction, the exact values from the
+    oracle's exact walk modulo primes. Nothing of the product is loaded."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     records = workload(0)
     import oracle
+    from oracle import exact_check
     threads = os.cpu_count() or 1
     kind = "reference" if oracle.have_ref("f64") else "port"
     run = (lambda: oracle.ref_walk("f64", P, Q, Z, N, H, records, threads=threads)) if kind == "reference" \
@@ -358,18 +517,13 @@ def main_reference(args):
         out = run()
         times.append(time.perf_counter() - t0)
     t = float(np.mean(times))
-    n_ver = None
-    try:
-        import torch
-        import cmfw
-        if torch.cuda.is_available():
-            # which ratio each limit came from (metadata for the exact check)
-            desc = cmfw.make_desc(P, Q, Z)
-            _, src = cmfw.walk("f64", desc, records, N, H, with_limit_src=True)
-            n_ver, _, _ = verify_counts(desc, records, out, src)
-    except Exception as e:  # the check needs the GPU; report the timing regardless
-        print(f"verification unavailable: {e}", file=sys.stderr)
-    value = (n_ver / t) if n_ver is not None else None
+    src, unattributed = reference_sources(records, out, threads)
+    t0 = time.perf_counter()
+    v = exact_check.verify(P, Q, Z, records, out, src, N, H, rtol=RTOL, threads=threads)
+    t_ver = time.perf_counter() - t0
+    n_ver = int(v["verified"].sum())
+    value = n_ver / t
+    valid = out["valid"] == 1
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "verified traj/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
@@ -377,9 +531,13 @@ def main_reference(args):
         "data": "synthetic (seeded std::mt19937_64 directions; no dataset)",
         "config": {"workload": "6F5 zeta delta search: x=1^6, y=2^5, z=1, rank 5, "
                                "dirs U{0..3}^11 != 0, N=1000, h=50", "n_traj_per_gpu": NTRAJ,
-                   "seed": SEED},
-        "n_traj": NTRAJ, "n_valid": int((out["valid"] == 1).sum()), "n_verified": n_ver,
-        "traj_per_s": NTRAJ / t,
+                   "seed": SEED, "variant": "f64",
+                   "verification": f"oracle exact walk modulo primes (CRT + rational reconstruction), rtol {RTOL}, "
+                                   "estimator of each limit from the oracle's restatement of the reference's "
+                                   "reduction"},
+        "n_traj": NTRAJ, "n_valid": int(valid.sum()), "n_verified": n_ver, "unattributed_rows": unattributed,
+        "traj_per_s": NTRAJ / t, "verify_s": t_ver,
+        "accuracy": accuracy(v["rel_err"], None, valid),
         "cpu_baseline": {"value": value, "unit": "verified traj/s", "cores": threads, "kind": kind,
                          "sample": f"the full batch ({NTRAJ} trajectories) per step"},
         "e2e": {"value": value, "unit": "verified traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

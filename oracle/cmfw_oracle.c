@@ -348,7 +348,9 @@ static int orc_forward_walk(const int *dir, const double *start, const orc_desc 
 /* Snapshot reduction                                                  */
 /* ------------------------------------------------------------------ */
 
-typedef struct { double L; int method; } limit_entry;
+/* One limit estimate and where it came from: the ratio M[i][c] / M[j][c]
+ * and the method (1 = Aitken, 0 = raw). */
+typedef struct { double L; int method, i, j, c; } limit_entry;
 
 /* cmf_pfq.cuh:385-460 — primary Aitken and raw ratio of M[0][d-1]/M[1][d-1],
  * then every other (i != j, column) ratio, capped at max_results. */
@@ -368,9 +370,9 @@ static int orc_limits(const snaps64 *s, int dim, limit_entry *res, int max_resul
                 if (fabs(den) > 1e-14 * sc) {
                     double dd = r2 - r3;
                     double L = r3 - dd * dd / den;
-                    if (isfinite(L) && n < max_results) res[n++] = (limit_entry){L, 1};
+                    if (isfinite(L) && n < max_results) res[n++] = (limit_entry){L, 1, 0, 1, c};
                 }
-                if (fabs(r3) > 1e-15 && n < max_results) res[n++] = (limit_entry){r3, 0};
+                if (fabs(r3) > 1e-15 && n < max_results) res[n++] = (limit_entry){r3, 0, 0, 1, c};
             }
         }
     }
@@ -390,9 +392,9 @@ static int orc_limits(const snaps64 *s, int dim, limit_entry *res, int max_resul
                 if (fabs(den) > 1e-14 * sc) {
                     double dd = r2 - r3;
                     double L = r3 - dd * dd / den;
-                    if (isfinite(L) && fabs(L) > 1e-15 && n < max_results) res[n++] = (limit_entry){L, 1};
+                    if (isfinite(L) && fabs(L) > 1e-15 && n < max_results) res[n++] = (limit_entry){L, 1, i, j, c};
                 }
-                if (fabs(r3) > 1e-15 && n < max_results) res[n++] = (limit_entry){r3, 0};
+                if (fabs(r3) > 1e-15 && n < max_results) res[n++] = (limit_entry){r3, 0, i, j, c};
             }
     return n;
 }
@@ -466,22 +468,32 @@ static double orc_kamidelta(const snaps64 *s, int dim, double Lt) {
 }
 
 /* Result fill shared by all variants (cmf_walk_f64.cu:122-153,
- * cmf_walk_df64.cu:333-348, cmf_walk_rns.cu:304-319). */
-static void orc_reduce(const snaps64 *s, int dim, double *limit, double *delta, double *p,
-                       double *q, double *precision, double *log_scale, int *n_limits) {
+ * cmf_walk_df64.cu:333-348, cmf_walk_rns.cu:304-319). *src (optional) gets
+ * the chosen estimate's source, (method << 12) | (i << 8) | (j << 4) | c, or
+ * -1 when there is none. */
+static void orc_reduce_src(const snaps64 *s, int dim, double *limit, double *delta, double *p,
+                           double *q, double *precision, double *log_scale, int *n_limits, int *src) {
     limit_entry lim[ORC_MAX_LIMITS];
     int n = orc_limits(s, dim, lim, ORC_MAX_LIMITS);
     *n_limits = n;
     double L = NAN;
+    int pick = -1;
     for (int i = 0; i < n; ++i)
-        if (lim[i].method == 1) { L = lim[i].L; break; }
-    if (isnan(L) && n > 0) L = lim[0].L;
+        if (lim[i].method == 1) { L = lim[i].L; pick = i; break; }
+    if (isnan(L) && n > 0) { L = lim[0].L; pick = 0; }
     *limit = L;
+    if (src)
+        *src = pick < 0 ? -1 : (lim[pick].method << 12) | (lim[pick].i << 8) | (lim[pick].j << 4) | lim[pick].c;
     *p = s->m[2].a[0][dim - 1];
     *q = s->m[2].a[1][dim - 1];
     *log_scale = s->ls[2];
     *precision = orc_precision(s, dim);
     *delta = orc_kamidelta(s, dim, L);
+}
+
+static void orc_reduce(const snaps64 *s, int dim, double *limit, double *delta, double *p,
+                       double *q, double *precision, double *log_scale, int *n_limits) {
+    orc_reduce_src(s, dim, limit, delta, p, q, precision, log_scale, n_limits, NULL);
 }
 
 static void orc_fill_invalid(double *limit, double *delta, double *p, double *q, double *precision,
@@ -494,9 +506,10 @@ static void set_threads(int threads) {
     if (threads > 0) omp_set_num_threads(threads);
 }
 
-/* cmf_walk_f64.cu:94-154 */
-int orc_walk_f64(int p, int q, double z, int N, int h, const orc_in *in, orc_out_f64 *out, int n,
-                 int fused, int threads) {
+/* cmf_walk_f64.cu:94-154; limit_src (optional, n ints) gets each row's
+ * estimate source (orc_reduce_src), -1 for invalid rows. */
+int orc_walk_f64_src(int p, int q, double z, int N, int h, const orc_in *in, orc_out_f64 *out, int n,
+                     int fused, int threads, int *limit_src) {
     orc_desc d = orc_make_desc(p, q, z);
     set_threads(threads);
 #pragma omp parallel for schedule(dynamic, 4)
@@ -504,15 +517,22 @@ int orc_walk_f64(int p, int q, double z, int N, int h, const orc_in *in, orc_out
         snaps64 s;
         orc_out_f64 *r = &out[i];
         int ok = orc_forward_walk(in[i].dir, in[i].start, &d, N, h, &s, fused);
+        int src = -1;
         r->valid = ok;
         if (!ok)
             orc_fill_invalid(&r->limit, &r->delta, &r->p, &r->q, &r->precision, &r->log_scale, &r->n_limits);
         else
-            orc_reduce(&s, d.rank, &r->limit, &r->delta, &r->p, &r->q, &r->precision, &r->log_scale,
-                       &r->n_limits);
+            orc_reduce_src(&s, d.rank, &r->limit, &r->delta, &r->p, &r->q, &r->precision, &r->log_scale,
+                           &r->n_limits, &src);
         r->elapsed_ms = 0.0;
+        if (limit_src) limit_src[i] = src;
     }
     return 0;
+}
+
+int orc_walk_f64(int p, int q, double z, int N, int h, const orc_in *in, orc_out_f64 *out, int n,
+                 int fused, int threads) {
+    return orc_walk_f64_src(p, q, z, N, h, in, out, n, fused, threads, NULL);
 }
 
 int orc_f64_snapshots(int p, int q, double z, int N, int h, const int *dir, const double *start,
@@ -918,4 +938,198 @@ int orc_rns_trace(int p, int q, double z, int N, int h, const int *dir, const do
             for (int j = 0; j < dim; ++j) out[(k * dim + i) * dim + j] = w->M.a[k][i][j];
     free(w);
     return ok;
+}
+
+/* ------------------------------------------------------------------ */
+/* Exact walk modulo primes                                            */
+/* ------------------------------------------------------------------ */
+
+/* The walk of cmf_pfq.cuh without rounding: every quantity of the f64 walk
+ * is a rational number (integer start, rational z = zn / zd), so the walk
+ * matrix is computed exactly in the field of residues modulo a prime m
+ * (one (trajectory, prime) pair per task). The steps are the reference's
+ * own formulas -- the column -d[i] / lead of D(theta) (cmf_pfq.cuh:146-181,
+ * scaled by zd, which leaves the column unchanged), the forward update and
+ * the row back-substitution of the inverse update (cmf_pfq.cuh:186-239),
+ * the evaluation point and denominator of each axis step
+ * (cmf_pfq.cuh:255-291), the path order (cmf_pfq.cuh:305-322) -- with
+ * divisions as multiplications by inverses modulo m. A prime for which a
+ * divisor (a * lead, or a row solve's scalar) vanishes is marked unusable;
+ * the rational value is then taken from the other primes. The projective
+ * normalisation is left out: it scales the whole matrix, and the ratios of
+ * entries that the limits are formed from do not depend on it.
+ *
+ * Arithmetic: Montgomery multiplication (P. L. Montgomery, Math. Comp. 44,
+ * 1985) with R = 2^32 for odd moduli below 2^31; inverses by Fermat's
+ * little theorem, a^(m-2). */
+typedef struct { uint32_t m, ninv, r2; } mont32;
+
+static mont32 mont_make(uint32_t m) {
+    mont32 M;
+    uint32_t inv = m; /* Newton's iteration for m^-1 mod 2^32 (m odd) */
+    for (int i = 0; i < 5; ++i) inv *= 2u - m * inv;
+    M.m = m;
+    M.ninv = 0u - inv;
+    uint64_t r1 = ((uint64_t)1 << 32) % m;
+    M.r2 = (uint32_t)((r1 * r1) % m);
+    return M;
+}
+static inline uint32_t mont_redc(uint64_t T, const mont32 *M) {
+    uint32_t u = (uint32_t)T * M->ninv;
+    uint64_t t = (T + (uint64_t)u * M->m) >> 32;
+    return t >= M->m ? (uint32_t)(t - M->m) : (uint32_t)t;
+}
+static inline uint32_t mont_mul(uint32_t a, uint32_t b, const mont32 *M) { return mont_redc((uint64_t)a * b, M); }
+static inline uint32_t mont_add(uint32_t a, uint32_t b, const mont32 *M) {
+    uint32_t r = a + b;
+    return r >= M->m ? r - M->m : r;
+}
+static inline uint32_t mont_sub(uint32_t a, uint32_t b, const mont32 *M) { return a >= b ? a - b : a + M->m - b; }
+static inline uint32_t mont_in(long long v, const mont32 *M) {
+    long long r = v % (long long)M->m;
+    if (r < 0) r += M->m;
+    return mont_mul((uint32_t)r, M->r2, M);
+}
+static inline uint32_t mont_out(uint32_t a, const mont32 *M) { return mont_redc(a, M); }
+static uint32_t mont_inv(uint32_t a, const mont32 *M) {
+    uint32_t r = mont_in(1, M), b = a;
+    for (uint32_t e = M->m - 2; e; e >>= 1) {
+        if (e & 1) r = mont_mul(r, b, M);
+        b = mont_mul(b, b, M);
+    }
+    return r;
+}
+
+/* Coefficients (ascending) of prod_j (theta + v_j) modulo m
+ * (cmf_pfq.cuh:127-141). */
+static void exact_poly(const uint32_t *v, int count, uint32_t *out, const mont32 *M) {
+    uint32_t one = mont_in(1, M);
+    for (int k = 0; k <= ORC_MAX_DIM; ++k) out[k] = 0;
+    out[0] = one;
+    for (int j = 0; j < count; ++j) {
+        for (int k = j + 1; k >= 1; --k) out[k] = mont_add(mont_mul(out[k], v[j], M), out[k - 1], M);
+        out[0] = mont_mul(out[0], v[j], M);
+    }
+}
+
+/* One trajectory modulo one prime; returns 1 if every divisor was
+ * invertible. snap gets entries (si, sc) and (sj, sc) at N-2h, N-h, N
+ * (plain residues, [3][2]). */
+static int exact_walk_one(const orc_desc *d, long long zn, long long zd, const int *dir, const double *start,
+                          int N, int h, uint32_t prime, int si, int sj, int sc, uint32_t snap[3][2]) {
+    const int dim = d->rank, p = d->p, q = d->q, naxes = d->naxes;
+    const mont32 Mo = mont_make(prime), *M = &Mo;
+    long long pos[ORC_MAX_AXES];
+    int maxabs = 0;
+    for (int a = 0; a < naxes; ++a) {
+        if (start[a] != floor(start[a]) || fabs(start[a]) >= 9.0e15) return 0;
+        if (abs(dir[a]) > 4096) return 0;
+        pos[a] = (long long)start[a];
+        maxabs = abs(dir[a]) > maxabs ? abs(dir[a]) : maxabs;
+    }
+    const uint32_t one = mont_in(1, M), zr = mont_in(zn, M), zdr = mont_in(zd, M);
+    uint32_t m[ORC_MAX_DIM][ORC_MAX_DIM];
+    for (int i = 0; i < dim; ++i)
+        for (int j = 0; j < dim; ++j) m[i][j] = (i == j) ? one : 0u;
+    const int cp1 = N - 2 * h, cp2 = N - h;
+    for (int step = 1; step <= N; ++step) {
+        for (int level = maxabs; level >= 1; --level)
+            for (int axis = naxes - 1; axis >= 0; --axis) {
+                if (abs(dir[axis]) < level) continue;
+                const int sign = dir[axis] > 0 ? 1 : -1;
+                const int is_x = axis < p;
+                const int inverse = is_x ? (sign < 0) : (sign > 0);
+                /* evaluation point and denominator (cmf_pfq.cuh:255-291) */
+                long long ev[ORC_MAX_AXES];
+                for (int a = 0; a < naxes; ++a) ev[a] = pos[a];
+                long long den;
+                if (is_x) {
+                    if (sign > 0) den = pos[axis];
+                    else { ev[axis] -= 1; den = pos[axis] - 1; }
+                } else {
+                    if (sign < 0) den = pos[axis] - 1;
+                    else { ev[axis] += 1; den = pos[axis]; }
+                }
+                uint32_t xv[ORC_MAX_AXES], yv[ORC_MAX_AXES], px[ORC_MAX_DIM + 1], py[ORC_MAX_DIM + 1];
+                for (int j = 0; j < p; ++j) xv[j] = mont_in(ev[j], M);
+                for (int i = 0; i < q; ++i) yv[i] = mont_in(ev[p + i] - 1, M);
+                exact_poly(xv, p, px, M);
+                exact_poly(yv, q, py, M);
+                /* zd * D(theta) = zd theta prod(theta + y_i - 1) - zn prod(theta + x_j) */
+                uint32_t dc[ORC_MAX_DIM + 2];
+                for (int k = 0; k <= dim; ++k) {
+                    uint32_t v = (k <= p) ? mont_sub(0, mont_mul(zr, px[k], M), M) : 0u;
+                    if (k >= 1 && k - 1 <= q) v = mont_add(v, mont_mul(zdr, py[k - 1], M), M);
+                    dc[k] = v;
+                }
+                const uint32_t lead = dc[dim], ar = mont_in(den, M);
+                const uint32_t al_ = mont_mul(ar, lead, M);
+                if (al_ == 0u) return 0;
+                const uint32_t inv_al = mont_inv(al_, M);
+                const uint32_t inva = mont_mul(inv_al, lead, M), il = mont_mul(inv_al, ar, M);
+                uint32_t col[ORC_MAX_DIM];
+                for (int i = 0; i < dim; ++i) col[i] = mont_sub(0, mont_mul(dc[i], il, M), M);
+                if (!inverse) {
+                    for (int r = 0; r < dim; ++r) {
+                        uint32_t dot = 0;
+                        for (int i = 0; i < dim; ++i) dot = mont_add(dot, mont_mul(m[r][i], col[i], M), M);
+                        for (int j = 0; j < dim - 1; ++j) m[r][j] = mont_add(m[r][j], mont_mul(m[r][j + 1], inva, M), M);
+                        m[r][dim - 1] = mont_add(m[r][dim - 1], mont_mul(dot, inva, M), M);
+                    }
+                } else {
+                    uint32_t be[ORC_MAX_DIM];
+                    be[dim - 1] = one;
+                    for (int j = dim - 2; j >= 0; --j) be[j] = mont_sub(0, mont_mul(be[j + 1], inva, M), M);
+                    uint32_t db = 0;
+                    for (int i = 0; i < dim; ++i) db = mont_add(db, mont_mul(be[i], col[i], M), M);
+                    const uint32_t sd = mont_add(one, mont_mul(db, inva, M), M);
+                    if (sd == 0u) return 0;
+                    const uint32_t isd = mont_inv(sd, M);
+                    for (int r = 0; r < dim; ++r) {
+                        uint32_t al[ORC_MAX_DIM];
+                        al[dim - 1] = 0;
+                        for (int j = dim - 2; j >= 0; --j) al[j] = mont_sub(m[r][j], mont_mul(al[j + 1], inva, M), M);
+                        uint32_t da = 0;
+                        for (int i = 0; i < dim; ++i) da = mont_add(da, mont_mul(al[i], col[i], M), M);
+                        const uint32_t t = mont_mul(mont_sub(m[r][dim - 1], mont_mul(da, inva, M), M), isd, M);
+                        for (int j = 0; j < dim; ++j) m[r][j] = mont_add(al[j], mont_mul(be[j], t, M), M);
+                    }
+                }
+                pos[axis] += sign;
+            }
+        const int s = step == cp1 ? 0 : step == cp2 ? 1 : step == N ? 2 : -1;
+        if (s >= 0) {
+            snap[s][0] = mont_out(m[si][sc], M);
+            snap[s][1] = mont_out(m[sj][sc], M);
+        }
+    }
+    return 1;
+}
+
+int orc_exact_residues(int p, int q, long long zn, long long zd, int N, int h, const orc_in *in, int n,
+                       const uint32_t *primes, int K, const int *pairs, uint32_t *res, uint8_t *ok, int threads) {
+    orc_desc d = orc_make_desc(p, q, zd != 0 ? (double)zn / (double)zd : 0.0);
+    const int dim = d.rank;
+    set_threads(threads);
+    const long long tasks = (long long)n * K;
+#pragma omp parallel for schedule(dynamic, 8)
+    for (long long g = 0; g < tasks; ++g) {
+        const int t = (int)(g / K), k = (int)(g % K);
+        int si = 0, sj = 1, sc = dim - 1;
+        if (pairs && pairs[t] >= 0) {
+            si = (pairs[t] >> 8) & 15;
+            sj = (pairs[t] >> 4) & 15;
+            sc = pairs[t] & 15;
+            if (si >= dim) si = dim - 1;
+            if (sj >= dim) sj = dim - 1;
+            if (sc >= dim) sc = dim - 1;
+        }
+        uint32_t snap[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+        int good = !(N <= 0 || h <= 0 || N - 2 * h <= 0) && (primes[k] & 1u) && primes[k] < (1u << 31);
+        if (good) good = exact_walk_one(&d, zn, zd, in[t].dir, in[t].start, N, h, primes[k], si, sj, sc, snap);
+        for (int s = 0; s < 3; ++s)
+            for (int e = 0; e < 2; ++e) res[(((size_t)t * 3 + s) * 2 + e) * K + k] = good ? snap[s][e] : 0u;
+        ok[(size_t)t * K + k] = (uint8_t)good;
+    }
+    return 0;
 }

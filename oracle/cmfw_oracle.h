@@ -48,6 +48,11 @@ void orc_mt64_stream(uint64_t seed, uint64_t *out, int n);
  * emits); 0 rounds every product and sum separately. threads <= 0: all. */
 int orc_walk_f64(int p, int q, double z, int N, int h, const orc_in *in,
                  orc_out_f64 *out, int n, int fused, int threads);
+/* orc_walk_f64 plus each row's limit source in limit_src (n ints):
+ * (method << 12) | (i << 8) | (j << 4) | c for the ratio M[i][c] / M[j][c]
+ * the limit came from (method 1 = Aitken, 0 = raw), -1 when none. */
+int orc_walk_f64_src(int p, int q, double z, int N, int h, const orc_in *in,
+                     orc_out_f64 *out, int n, int fused, int threads, int *limit_src);
 int orc_walk_df64(int p, int q, double z, int N, int h, const orc_in *in,
                   orc_out *out, int n, int fused, int threads);
 int orc_walk_rns(int p, int q, double z, int N, int h, const orc_in *in,
@@ -61,6 +66,15 @@ int orc_rns_trace(int p, int q, double z, int N, int h, const int *dir,
                   const double *start, int n_primes, int steps, int fused,
                   uint32_t *out, double *log_scale_out);
 void orc_rns_moduli(uint32_t *out, int n);
+
+/* Exact walk modulo primes (odd, below 2^31), z = zn / zd: residues of the
+ * entries (i, c) and (j, c) of the walk matrix at depths N-2h, N-h, N, with
+ * (i, j, c) from pairs[t] = (i << 8) | (j << 4) | c (NULL or -1: 0, 1,
+ * rank-1). res: n * 3 * 2 * K, index ((t * 3 + depth) * 2 + entry) * K + k;
+ * ok: n * K, 0 where a divisor vanished modulo that prime. */
+int orc_exact_residues(int p, int q, long long zn, long long zd, int N, int h,
+                       const orc_in *in, int n, const uint32_t *primes, int K,
+                       const int *pairs, uint32_t *res, uint8_t *ok, int threads);
 
 /* Companion column at a position (for kernel-level checks). */
 int orc_column(const double *pos, double z, int dim, int p, int q,

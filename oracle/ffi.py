@@ -19,13 +19,16 @@ assert IN_DTYPE.itemsize == 192 and OUT_DTYPE.itemsize == 56 and OUT_F64_DTYPE.i
 _c_int, _c_dbl, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
 
-def build(with_ref=None):
-    """Compile liboracle.so (and the reference checkers when its sources exist)."""
+def build(with_ref=None, ref_root=None):
+    """Compile liboracle.so, and the reference checkers (oracle/_ref) from the
+    reference checkout named by ref_root or CMFW_REF_ROOT when it exists."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    ref_root = os.environ.get("CMFW_REF_ROOT", "/root/reference")
+    ref_root = ref_root or os.environ.get("CMFW_REF_ROOT")
     if with_ref is None:
-        with_ref = os.path.isdir(os.path.join(ref_root, "cuda"))
+        with_ref = bool(ref_root) and os.path.isdir(os.path.join(ref_root, "cuda"))
     if with_ref:
+        if not ref_root:
+            raise RuntimeError("CMFW_REF_ROOT must name the reference checkout to build oracle/_ref")
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={ref_root}"], check=True)
 
 
@@ -40,6 +43,9 @@ def _oracle():
         lib = ctypes.CDLL(ORACLE_LIB)
         walk_args = [_c_int, _c_int, _c_dbl, _c_int, _c_int, _vp, _vp, _c_int]
         lib.orc_walk_f64.argtypes = walk_args + [_c_int, _c_int]
+        lib.orc_walk_f64_src.argtypes = walk_args + [_c_int, _c_int, _vp]
+        lib.orc_exact_residues.argtypes = [_c_int, _c_int, ctypes.c_longlong, ctypes.c_longlong, _c_int,
+                                           _c_int, _vp, _c_int, _vp, _c_int, _vp, _vp, _vp, _c_int]
         lib.orc_walk_df64.argtypes = walk_args + [_c_int, _c_int]
         lib.orc_walk_rns.argtypes = walk_args + [_c_int, _c_int, _c_int]
         lib.orc_make_inputs.argtypes = [_c_int, _c_int, _c_int, _c_int, _c_int, _vp]
@@ -88,6 +94,38 @@ def walk(variant, p, q, z, N, h, inputs, n_primes=8, fused=False, threads=0):
     else:
         raise ValueError(variant)
     return out
+
+
+def walk_f64_src(p, q, z, N, h, inputs, fused=False, threads=0):
+    """The f64 oracle walk and, per row, the source of its limit: (method
+    << 12) | (i << 8) | (j << 4) | c for the ratio M[i][c] / M[j][c] chosen
+    by the reference's reduction (method 1 = Aitken, 0 = raw), -1 when the
+    row has no limit."""
+    inputs = np.ascontiguousarray(inputs, dtype=IN_DTYPE)
+    n = len(inputs)
+    out = np.zeros(n, dtype=OUT_F64_DTYPE)
+    src = np.full(n, -1, dtype=np.int32)
+    _oracle().orc_walk_f64_src(p, q, z, N, h, _ptr(inputs), _ptr(out), n, int(fused), threads, _ptr(src))
+    return out, src
+
+
+def exact_residues(p, q, zn, zd, N, h, inputs, primes, pairs=None, threads=0):
+    """Exact walk modulo each prime (odd, below 2^31): residues of the
+    entries (i, c) and (j, c) of the walk matrix at depths N-2h, N-h, N as
+    an array [n, 3, 2, K], and a per-prime usability mask [n, K]."""
+    inputs = np.ascontiguousarray(inputs, dtype=IN_DTYPE)
+    primes = np.ascontiguousarray(primes, dtype=np.uint32)
+    n, K = len(inputs), len(primes)
+    res = np.zeros((n, 3, 2, K), dtype=np.uint32)
+    ok = np.zeros((n, K), dtype=np.uint8)
+    pr = None
+    if pairs is not None:
+        pr = np.ascontiguousarray(pairs, dtype=np.int32)
+        assert len(pr) == n
+    if n and K:
+        _oracle().orc_exact_residues(p, q, int(zn), int(zd), N, h, _ptr(inputs), n, _ptr(primes), K,
+                                     None if pr is None else _ptr(pr), _ptr(res), _ptr(ok), threads)
+    return res, ok.astype(bool)
 
 
 def _dir_start(dir_, start):
@@ -198,3 +236,30 @@ def ref_rns_moduli(n=64):
     out = np.zeros(n, dtype=np.uint32)
     _ref("rns").ref_rns_primes(_ptr(out), n)
     return out
+
+
+# ---------------------------------------------------------------------------
+# The reference's own CUDA kernels built for sm_100a (oracle/_ref, comparison
+# arm of the benchmark).
+# ---------------------------------------------------------------------------
+def have_ref_gpu(variant="f64"):
+    return os.path.exists(os.path.join(REF_DIR, f"libref_gpu_{variant}.so"))
+
+
+def ref_gpu_launch(variant, p, q, z, N, h, d_in, d_out, n, block=0, stream=0, n_primes=8):
+    """Launch the reference kernel walk_kernel_<variant> on device buffers
+    (integer device addresses of n reference input / result records) on
+    `stream`; block 0 = the reference's default (256, RNS 128)."""
+    key = ("gpu", variant)
+    if key not in _ref_libs:
+        lib = ctypes.CDLL(os.path.join(REF_DIR, f"libref_gpu_{variant}.so"))
+        args = [_vp, _vp, _c_int, _c_int, _c_dbl, _c_int, _c_int, _c_int, _c_int]
+        fn = getattr(lib, f"ref_gpu_{variant}_launch")
+        fn.argtypes = args + ([_c_int] if variant == "rns" else []) + [_vp]
+        _ref_libs[key] = lib
+    fn = getattr(_ref_libs[key], f"ref_gpu_{variant}_launch")
+    block = block or (128 if variant == "rns" else 256)
+    extra = [n_primes] if variant == "rns" else []
+    rc = fn(_vp(d_in), _vp(d_out), p, q, z, N, h, n, block, *extra, _vp(stream))
+    if rc != 0:
+        raise RuntimeError(f"reference {variant} kernel launch failed: CUDA error {rc}")

@@ -68,6 +68,9 @@ struct ChunkArgs {
     int *parts_e;                     // nslots x 3 their exponents
     unsigned long long *parts_fail;   // nslots earliest failure keys
     int nslots;
+    // CTAs that survivors walked in parts are shared out over: one per SM,
+    // whatever the kernel's occupancy, and at most 32 * kLaneItems
+    int part_budget;
     int prefix_steps;
 };
 
@@ -427,10 +430,11 @@ __device__ __forceinline__ void run_geometry(int N, int h, int np, int rt, int g
 }
 
 // CTAs that walk one trajectory together, at most, and the survivors per
-// lane of the warp that shares out the parts (32 x 10 covers the largest
-// grid, two CTAs per SM).
+// lane of the warp that shares out the parts: the host caps the part budget
+// at 32 x kLaneItems, so the warp sees every survivor of a balanced batch.
 constexpr int kMaxParts = 16;
 constexpr int kLaneItems = 10;
+constexpr int kMaxPartBudget = 32 * kLaneItems;
 
 __device__ __forceinline__ double ldcg_d(const double *p) { return __ldcg(p); }
 __device__ __forceinline__ dd ldcg_d(const dd *p) { return dd{__ldcg(&p->hi), __ldcg(&p->lo)}; }
@@ -478,15 +482,19 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
     const int naxes = P + Q;
     if (tid == 0) s_K = make_step_const(P, Q, DIM, W.z);
 
-    // Parts per trajectory. With no more survivors than CTAs, every
-    // survivor b gets NP_b = min(kMaxParts, ceil(w_b / t)) CTAs, w_b = its
-    // axis steps per lattice step (its walk's cost), t the smallest work
-    // per CTA (in sixteenths) whose parts fit the grid: long walks get more
-    // CTAs, so the CTAs end at about the same time. Survivors take
-    // consecutive CTAs in list order; a CTA walks one part and is done.
-    // With more survivors than CTAs, every survivor is one CTA's and the
-    // CTAs stride over the list. Warp 0 finds this CTA's part; the values
-    // are kept in shared memory, like the run geometry below.
+    // Parts per trajectory. With no more survivors than the part budget B
+    // (one CTA per SM), every survivor b gets NP_b = min(kMaxParts,
+    // ceil(w_b / t)) CTAs, w_b = its axis steps per lattice step (its
+    // walk's cost), t the smallest work per CTA (in sixteenths) whose parts
+    // fit B: long walks get more CTAs, so the CTAs end at about the same
+    // time. Survivors take consecutive CTAs in list order; a CTA walks one
+    // part and is done (CTAs past the parts exit). With more survivors than
+    // B, every survivor is one CTA's and the CTAs stride over the list.
+    // B is fixed by the SM count alone, not by how many CTAs of this build
+    // fit an SM: NP_b, hence the run geometry and the association of the
+    // product (and so every rounding), depend on the batch and the device
+    // only. Warp 0 finds this CTA's part; the values are kept in shared
+    // memory, like the run geometry below.
     __shared__ int s_count, s_bal, s_b0, s_part0, s_np0, s_first0;
     // The filter kernel is launched before this one with programmatic
     // stream serialisation: wait (in hardware) until it has finished and
@@ -494,7 +502,7 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
     cudaGridDependencySynchronize();
     if (tid < 32) {
         const int count = *C.count;
-        const int Gr = min((int)gridDim.x, C.nslots);
+        const int Gr = min(min((int)gridDim.x, C.nslots), min(C.part_budget, kMaxPartBudget));
         const bool bal = count > 0 && count <= Gr;
         int b0 = -1, part0 = 0, np0 = 1, first0 = 0;
         if (bal) {
@@ -961,6 +969,7 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     C.parts_e = (int *)(p + lay.parts_e);
     C.parts_fail = (unsigned long long *)(p + lay.parts_fail);
     C.nslots = nslots;
+    C.part_budget = std::min(device_sms(), kMaxPartBudget);
     C.prefix_steps = prefix_steps;
     const int NT = chunk_threads(dim);
     const size_t shmem = chunk_smem_bytes<typename A::Combine::T>(dim);

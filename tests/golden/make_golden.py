@@ -85,7 +85,9 @@ def reference_runs():
 
 
 if __name__ == "__main__":
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CMFW_REF_ROOT")
+    if not ref_root:
+        sys.exit("usage: make_golden.py <reference checkout> (or set CMFW_REF_ROOT)")
     published(ref_root)
     reference_runs()
     print("golden fixtures written to", HERE)

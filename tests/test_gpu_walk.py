@@ -72,6 +72,42 @@ def _limit_parity(desc, recs, g, src, o, N, h, rtol=1e-9):
     return len(far)
 
 
+def _tail_parity(g, o, same_tol, tol, min_rows=0, lim_tol=1e-9):
+    """precision and delta (cmf_pfq.cuh:476-552) against the oracle, on the
+    valid rows whose limit the two agree on within lim_tol (the same
+    estimator). Both fields
+    take logs of differences of nearly converged ratios, so:
+      * which rows are NaN or infinite must agree exactly;
+      * values are compared where they are well conditioned -- the ratios at
+        N and N-h differ by more than 1e-6 relative (the oracle's precision
+        says how much), so a relative error e of the walk moves precision
+        by about e * 1e6 / ln 10 digits -- and where the GPU's p/q agree with
+        the oracle's within same_tol: there, within tol (precision, digits)
+        and tol * max(1, |delta|) (delta) on at least 95% of the rows.
+    Returns the number of value-compared rows."""
+    m = (g["valid"] == 1) & (o["valid"] == 1)
+    with np.errstate(invalid="ignore"):
+        lim_same = (np.isnan(g["limit"]) & np.isnan(o["limit"])) | \
+            (np.abs(g["limit"] - o["limit"]) <= lim_tol * np.abs(o["limit"]))
+    m &= lim_same
+    for k in ("precision", "delta"):
+        assert np.array_equal(np.isnan(g[k][m]), np.isnan(o[k][m])), k
+        assert np.array_equal(np.isinf(g[k][m]), np.isinf(o[k][m])), k
+    with np.errstate(invalid="ignore", divide="ignore"):
+        rel_pq = np.abs(g["p"] / g["q"] - o["p"] / o["q"]) / np.abs(o["p"] / o["q"])
+        scale = np.log10(np.maximum(np.abs(o["limit"]), 1e-300))
+        cond = m & np.isfinite(o["precision"]) & (o["precision"] < 6.0 - scale) & (rel_pq <= same_tol)
+    cond &= np.isfinite(o["delta"])
+    n = int(cond.sum())
+    assert n >= min_rows, n
+    if n:
+        dp = np.abs(g["precision"][cond] - o["precision"][cond])
+        dd = np.abs(g["delta"][cond] - o["delta"][cond]) / np.maximum(1.0, np.abs(o["delta"][cond]))
+        assert (dp <= tol).mean() >= 0.95, ("precision", float(dp.max()))
+        assert (dd <= tol).mean() >= 0.95, ("delta", float(dd.max()))
+    return n
+
+
 @pytest.mark.parametrize("p,q", FAMILIES)
 @pytest.mark.parametrize("z,mode", [(0.5, 0), (1.0, 0), (0.5, 1)])
 @pytest.mark.parametrize("flags", [0, cmfw.F_SEQUENTIAL])
@@ -90,6 +126,39 @@ def test_f64_matches_oracle(cuda, p, q, z, mode, flags):
     for k in ("p", "q", "log_scale"):
         _close_fraction(g[k][m], o[k][m], 1e-9, k)
     assert (g["n_limits"][m] == o["n_limits"][m]).mean() >= 0.8
+    _tail_parity(g, o, 1e-11, 1e-4)
+
+
+def test_f64_cfg2_batch_matches_oracle(cuda):
+    """The benchmark's own batch (6F5 zeta, 10,000 directions U{0..3}^11,
+    seed 20261203, N = 1000, h = 50): validity identical row for row, limit /
+    p / q / log_scale within the oracle bars, precision and delta by their
+    NaN pattern and where conditioned."""
+    import cmfw.workloads as wl
+    recs = wl.zeta_directions(6, 5, 10000, 20261203)
+    desc = cmfw.make_desc(6, 5, 1.0)
+    g, src = cmfw.walk("f64", desc, recs, 1000, 50, with_limit_src=True)
+    o = oracle.walk("f64", 6, 5, 1.0, 1000, 50, recs, fused=True)
+    np.testing.assert_array_equal(g["valid"], o["valid"])
+    m = g["valid"] == 1
+    assert 30 <= m.sum() <= 100
+    _limit_parity(desc, recs, g, src, o, 1000, 50)
+    for k in ("p", "q", "log_scale"):
+        _close_fraction(g[k][m], o[k][m], 1e-9, k)
+    _tail_parity(g, o, 1e-11, 1e-4)
+
+
+def test_df64_tail_matches_oracle(cuda):
+    """df64 (float-float runs): precision and delta against the oracle's f64
+    walk, NaN pattern exactly, values where conditioned (a float-float walk
+    is good to about 1e-9 relative, so the bar is 1e-3)."""
+    p, q = 4, 3
+    recs = oracle.make_inputs(p, q, 600, 0, False)[:300]
+    desc = cmfw.make_desc(p, q, 0.5)
+    g = cmfw.walk("df64", desc, recs, 1000, 50)
+    o = oracle.walk("f64", p, q, 0.5, 1000, 50, recs, fused=True)
+    np.testing.assert_array_equal(g["valid"], o["valid"])
+    _tail_parity(g, o, 1e-8, 1e-3, lim_tol=1e-6)
 
 
 @pytest.mark.parametrize("p,q", [(6, 5), (8, 7), (3, 2)])
