@@ -123,6 +123,14 @@ typedef struct {
  * amplified when the runs are multiplied back together, so results may be
  * less accurate than the sequential walk's. */
 #define CMFW_F_PLAIN_RUNS 0x8
+/* f64 / df64 chunked walk: walk every trajectory that passes the filter in
+ * one CTA, whatever the batch. By default a batch with fewer survivors than
+ * SMs spreads each survivor over several CTAs, in numbers that depend on the
+ * whole batch; that changes the association of the walk's product and so
+ * its rounding (in f64 by about an ulp, in df64 visibly on ill-conditioned
+ * walks). With this flag a trajectory's result is the same bits in every
+ * batch (on a given GPU), at the cost of latency for small batches. */
+#define CMFW_F_BATCH_INVARIANT 0x10
 
 /* ---- descriptors and library state -------------------------------- */
 
@@ -208,6 +216,28 @@ cmfw_status cmfw_rns_trace(const cmfw_desc *desc, const cmfw_traj_in *d_in, int 
 cmfw_status cmfw_exact_residues(const cmfw_desc *desc, const cmfw_traj_in *d_in, int n_traj,
                                 int N, int h, const uint32_t *d_primes, int K, const int *d_pairs,
                                 uint32_t *d_res, uint8_t *d_prime_ok, void *stream);
+/* The exact ratios of cmfw_exact_residues' output, reconstructed on the
+ * device (no reference counterpart: the reference's CRT uses two primes and
+ * rounds, cmf_walk_rns.cu:225-251). Per trajectory t and depth s (task
+ * 3 t + s): the rational n / d whose residues modulo d_primes[0..K) are
+ * res[t][s][0][k] / res[t][s][1][k], over the primes with prime_ok set and a
+ * non-zero denominator residue; res and prime_ok are laid out with `stride`
+ * primes per trajectory (K <= stride: a prefix of the walked primes may be
+ * used). One warp per task: Garner's mixed-radix CRT with a lane per prime,
+ * rational reconstruction by the half-extended Euclidean algorithm to
+ * Wang's bound, and a check on the last 4 usable primes, which the fit
+ * leaves out. Primes must be odd and in (2^30, 2^31). Outputs per task: the
+ * magnitudes of n and d as little-endian 32-bit words in
+ * d_num / d_den[task * cmfw_exact_recon_words(K) ...], their word counts, the
+ * sign of n, and d_status: 0 = n / d, 1 = the denominator vanishes modulo
+ * every usable prime (exactly zero), 2 = undetermined (too few primes for
+ * its size, or the check failed: add primes), 3 = no usable prime (the
+ * exact walk is singular). */
+int cmfw_exact_recon_words(int K);
+cmfw_status cmfw_exact_reconstruct(const uint32_t *d_res, const uint8_t *d_prime_ok, const uint32_t *d_primes,
+                                   int n_traj, int stride, int K, uint32_t *d_num, uint32_t *d_den,
+                                   int *d_num_words, int *d_den_words, int8_t *d_sign, uint8_t *d_status,
+                                   void *stream);
 
 /* ---- mixed batches (no reference counterpart: the reference walks one
  * family at one depth per program run, cmf_walk_f64.cu:156-305) ---------
@@ -317,6 +347,24 @@ cmfw_status cmfw_mlp_score_candidates(cmfw_mlp *mlp, uint64_t seed, long long fi
 cmfw_status cmfw_mlp_score_candidates_fused(cmfw_mlp *mlp, uint64_t seed, long long first, long long n,
                                             int naxes, int lo, int hi, int family, float *d_scores,
                                             void *stream);
+/* The same network on candidates d_idx[0..n) of the generator (any subset,
+ * e.g. the survivors of cmfw_filter_candidates), scores into d_scores[0..n).
+ * No reference counterpart (the learned proposal is this project's). */
+cmfw_status cmfw_mlp_score_indices(cmfw_mlp *mlp, uint64_t seed, const long long *d_idx, long long n, int naxes,
+                                   int lo, int hi, int family, float *d_scores, void *stream);
+/* The chunked walk's singularity filter on candidates first .. first+n-1
+ * of the generator (start h_start[0..naxes), naxes <= 15): the position-only
+ * tests of the first `steps` lattice steps (the walk itself uses 1), no
+ * matrix work. The indices of the candidates that pass go to d_idx (at most
+ * cap, in no particular order) and their number to *d_count (which may
+ * exceed cap: then only cap were written); d_count is cleared on the
+ * stream first. Every other candidate is an invalid walk (the reference's
+ * tests of cmf_pfq.cuh:164-174, 193 and 225-232 on its first steps); with
+ * N - 2h <= 0 none pass. No reference counterpart (the reference walks every
+ * trajectory). */
+cmfw_status cmfw_filter_candidates(const cmfw_desc *desc, uint64_t seed, long long first, long long n, int lo,
+                                   int hi, const double *h_start, int N, int h, int steps, long long *d_idx,
+                                   long long cap, unsigned long long *d_count, void *stream);
 /* Records of the candidates d_idx[0..n) of the same generator, start d_start. */
 cmfw_status cmfw_candidate_records(uint64_t seed, const long long *d_idx, int n, int naxes, int lo, int hi,
                                    const double *d_start, cmfw_traj_in *d_out, void *stream);

@@ -33,6 +33,7 @@ F_DF64_COMPAT = 0x1
 F_UNFUSED_COLUMN = 0x2
 F_SEQUENTIAL = 0x4
 F_PLAIN_RUNS = 0x8
+F_BATCH_INVARIANT = 0x10
 NOALLOC_SCRATCH_BYTES = 32 << 20  # CMFW_NOALLOC_SCRATCH_BYTES
 
 VARIANTS = {"f64": 0, "df64": 1, "rns": 2}
@@ -41,13 +42,15 @@ VARIANTS = {"f64": 0, "df64": 1, "rns": 2}
 EXPORTS = [
     "cmfw_version", "cmfw_last_error", "cmfw_make_desc", "cmfw_check_desc",
     "cmfw_walk_workspace_bytes", "cmfw_walk_f64", "cmfw_walk_f64_noalloc", "cmfw_walk_df64", "cmfw_walk_rns",
-    "cmfw_rns_trace", "cmfw_exact_residues", "cmfw_reference_inputs", "cmfw_mt64_fill",
+    "cmfw_rns_trace", "cmfw_exact_residues", "cmfw_exact_recon_words", "cmfw_exact_reconstruct",
+    "cmfw_reference_inputs", "cmfw_mt64_fill",
     "cmfw_mt64_fill_at", "cmfw_walk_host", "cmfw_pipe_peak", "cmfw_device_banner", "cmfw_device_meminfo",
     "cmfw_mixed_workspace_bytes", "cmfw_walk_mixed", "cmfw_mixed_autotune", "cmfw_mixed_graph_create",
     "cmfw_mixed_graph_launch", "cmfw_mixed_graph_destroy",
     "cmfw_mlp_create", "cmfw_mlp_destroy", "cmfw_mlp_param_count", "cmfw_mlp_get_params", "cmfw_mlp_set_params",
     "cmfw_mlp_forward", "cmfw_mlp_gradients", "cmfw_mlp_train_step", "cmfw_mlp_status",
-    "cmfw_mlp_score_candidates", "cmfw_mlp_score_candidates_fused", "cmfw_candidate_records", "cmfw_select_top",
+    "cmfw_mlp_score_candidates", "cmfw_mlp_score_candidates_fused", "cmfw_mlp_score_indices",
+    "cmfw_filter_candidates", "cmfw_candidate_records", "cmfw_select_top",
 ]
 
 
@@ -107,6 +110,8 @@ def lib():
         L.cmfw_walk_rns.argtypes = [P(Desc), vp, vp, ci, ci, ci, ci, P(Launch), vp]
         L.cmfw_rns_trace.argtypes = [P(Desc), vp, ci, ci, ci, ci, ci, ci, vp, vp, vp]
         L.cmfw_exact_residues.argtypes = [P(Desc), vp, ci, ci, ci, vp, ci, vp, vp, vp, vp]
+        L.cmfw_exact_recon_words.argtypes = [ci]
+        L.cmfw_exact_reconstruct.argtypes = [vp, vp, vp, ci, ci, ci, vp, vp, vp, vp, vp, vp, vp]
         L.cmfw_reference_inputs.argtypes = [ci, ci, ci, ci, ci, vp]
         L.cmfw_mt64_fill.argtypes = [ctypes.c_uint64, vp, cs]
         L.cmfw_mt64_fill.restype = None
@@ -139,6 +144,8 @@ def lib():
         L.cmfw_mlp_status.argtypes = [vp]
         L.cmfw_mlp_score_candidates.argtypes = [vp, u64, ll, ll, ci, ci, ci, ci, vp, vp]
         L.cmfw_mlp_score_candidates_fused.argtypes = [vp, u64, ll, ll, ci, ci, ci, ci, vp, vp]
+        L.cmfw_mlp_score_indices.argtypes = [vp, u64, vp, ll, ci, ci, ci, ci, vp, vp]
+        L.cmfw_filter_candidates.argtypes = [P(Desc), u64, ll, ll, ci, ci, vp, ci, ci, ci, vp, ll, vp, vp]
         L.cmfw_candidate_records.argtypes = [u64, vp, ci, ci, ci, ci, vp, vp, vp]
         L.cmfw_select_top.argtypes = [vp, ll, ll, vp, ci, P(ci), vp]
         _lib = L

@@ -172,6 +172,64 @@ def exact_residues(desc, records, N, h, primes, pairs=None, d_in=None):
     return d_res.cpu().numpy().view(np.uint32), d_ok.cpu().numpy().astype(bool)
 
 
+def exact_residues_device(desc, d_in, n, N, h, primes, pairs=None):
+    """cmfw_exact_residues into device tensors: (d_res [n, 3, 2, K] int32
+    view of uint32, d_ok [n, K] uint8, d_primes)."""
+    torch = _torch()
+    primes = np.ascontiguousarray(primes, dtype=np.uint32)
+    K = len(primes)
+    d_primes = torch.from_numpy(primes.view(np.int32)).cuda()
+    d_res = torch.zeros((max(n, 1), 3, 2, K), dtype=torch.int32, device="cuda")
+    d_ok = torch.zeros((max(n, 1), K), dtype=torch.uint8, device="cuda")
+    d_pairs = None
+    if pairs is not None:
+        d_pairs = torch.from_numpy(np.ascontiguousarray(pairs, dtype=np.int32)).cuda()
+    if n:
+        check(lib().cmfw_exact_residues(
+            ctypes.byref(desc), ctypes.c_void_p(d_in.data_ptr()), n, N, h,
+            ctypes.c_void_p(d_primes.data_ptr()), K,
+            ctypes.c_void_p(d_pairs.data_ptr()) if d_pairs is not None else None,
+            ctypes.c_void_p(d_res.data_ptr()), ctypes.c_void_p(d_ok.data_ptr()), _stream_handle(None)))
+    return d_res, d_ok, d_primes
+
+
+def exact_reconstruct(d_res, d_ok, d_primes, n, K):
+    """cmfw_exact_reconstruct over the first K primes of device residues
+    (d_res [n, 3, 2, stride]): per (trajectory, depth) a status (0 fraction,
+    1 zero denominator, 2 undetermined, 3 singular) and the fraction as a
+    Python (numerator, denominator) pair where the status is 0."""
+    torch = _torch()
+    stride = int(d_res.shape[-1])
+    W = lib().cmfw_exact_recon_words(int(K))
+    T = 3 * n
+    d_num = torch.zeros((max(T, 1), W), dtype=torch.int32, device="cuda")
+    d_den = torch.zeros((max(T, 1), W), dtype=torch.int32, device="cuda")
+    d_ln = torch.zeros(max(T, 1), dtype=torch.int32, device="cuda")
+    d_ld = torch.zeros(max(T, 1), dtype=torch.int32, device="cuda")
+    d_sg = torch.zeros(max(T, 1), dtype=torch.int8, device="cuda")
+    d_st = torch.zeros(max(T, 1), dtype=torch.uint8, device="cuda")
+    if n:
+        check(lib().cmfw_exact_reconstruct(
+            ctypes.c_void_p(d_res.data_ptr()), ctypes.c_void_p(d_ok.data_ptr()),
+            ctypes.c_void_p(d_primes.data_ptr()), int(n), stride, int(K),
+            ctypes.c_void_p(d_num.data_ptr()), ctypes.c_void_p(d_den.data_ptr()),
+            ctypes.c_void_p(d_ln.data_ptr()), ctypes.c_void_p(d_ld.data_ptr()),
+            ctypes.c_void_p(d_sg.data_ptr()), ctypes.c_void_p(d_st.data_ptr()), _stream_handle(None)))
+    st = d_st[:T].cpu().numpy()
+    ln, ld, sg = d_ln[:T].cpu().numpy(), d_ld[:T].cpu().numpy(), d_sg[:T].cpu().numpy()
+    good = np.nonzero(st == 0)[0]
+    fracs = [None] * T
+    if len(good):
+        gi = torch.from_numpy(good).cuda()
+        nums = d_num[gi].cpu().numpy().view(np.uint32)
+        dens = d_den[gi].cpu().numpy().view(np.uint32)
+        for r, t in enumerate(good):
+            num = int.from_bytes(nums[r, :ln[t]].tobytes(), "little")
+            den = int.from_bytes(dens[r, :ld[t]].tobytes(), "little")
+            fracs[t] = (-num if sg[t] < 0 else num, den)
+    return st.reshape(n, 3), [fracs[3 * i:3 * i + 3] for i in range(n)]
+
+
 def pipe_peak(pipe):
     """Measured FMA throughput (tera-ops/s, FMA = 2) of pipe 0 FP64, 1 FP32, 2 INT32."""
     v = ctypes.c_double(0)

@@ -1,11 +1,14 @@
 """Exact verification of floating-point walk results.
 
 The GPU exact walk (cmfw_exact_residues) keeps the walk product as rational
-residues modulo K primes. Here the residues of two entries of one column at
-the three snapshot depths become exact rationals: per prime the ratio
-a * b^-1, Chinese remaindering over the primes, then rational reconstruction
-(Wang's half-extended-Euclid bound sqrt(P/2)) checked against held-out
-primes. When the check fails the walk is rerun with four times the primes.
+residues modulo K primes. The residues of two entries of one column at the
+three snapshot depths become exact rationals on the device
+(cmfw_exact_reconstruct: per prime the ratio a * b^-1, Garner's
+Chinese remaindering with a warp lane per prime, rational reconstruction to
+Wang's half-extended-Euclid bound sqrt(P/2), checked against held-out
+primes); the host only turns the resulting words into Python integers. A
+reconstruction that the primes do not determine is retried on a longer
+prefix of the walked primes, then with four times the primes walked.
 
 "Verified" means: the floating-point walk is valid, the exact walk is valid,
 and the reported limit agrees with the exact value of the same estimator
@@ -126,40 +129,41 @@ def exact_ratios(desc, records, N, h, pairs=None, K0=64, K_max=4096):
     where the denominator is exactly zero), or None where the exact walk is
     invalid (a divisor vanished for every prime).
     """
+    torch = api._torch()
     n = len(records)
     ratios = [None] * n
     K_used = np.zeros(n, dtype=np.int64)
     todo = np.arange(n)
     K_run = K0
     while len(todo) and K_run <= K_max:
-        # one GPU run with K_run primes; reconstruction tries growing prefixes
+        # one exact walk with K_run primes; reconstructions on growing prefixes
         primes = primes_below_2_31(K_run)
         sub = records[todo]
         sub_pairs = None if pairs is None else np.asarray(pairs)[todo]
-        res, ok = api.exact_residues(desc, sub, N, h, primes.astype(np.uint32), sub_pairs)
-        retry = []
-        for li, t in enumerate(todo):
-            if not ok[li].any():
-                ratios[t] = None
-                K_used[t] = K_run
-                continue
-            K = min(64, K_run)
-            while True:
-                rs = []
-                for s in range(3):
-                    r = _ratio_from_residues(res[li, s, 0, :K], res[li, s, 1, :K], ok[li, :K], primes[:K])
-                    if r is None:
-                        break
-                    rs.append(r)
-                if len(rs) == 3 or K >= K_run:
-                    break
-                K = min(K * 2, K_run)
-            if len(rs) < 3:
-                retry.append(t)
-            else:
-                ratios[t] = rs
-                K_used[t] = K
-        todo = np.array(retry, dtype=np.int64)
+        d_in = api.to_device(sub)
+        d_res, d_ok, d_primes = api.exact_residues_device(desc, d_in, len(sub), N, h, primes, sub_pairs)
+        pending = np.arange(len(todo))
+        K = min(64, K_run)
+        while len(pending):
+            sel = torch.from_numpy(pending).cuda()
+            st, fr = api.exact_reconstruct(d_res[sel].contiguous(), d_ok[sel].contiguous(), d_primes,
+                                           len(pending), K)
+            left = []
+            for r, li in enumerate(pending):
+                t = todo[li]
+                if (st[r] == 3).all():
+                    ratios[t] = None  # singular for every prime: the exact walk is invalid
+                    K_used[t] = K
+                elif (st[r] == 2).any():
+                    left.append(li)
+                else:
+                    ratios[t] = ["inf" if st[r, k] == 1 else Fraction(*fr[r][k]) for k in range(3)]
+                    K_used[t] = K
+            pending = np.array(left, dtype=np.int64)
+            if K >= K_run:
+                break
+            K = min(K * 2, K_run)
+        todo = todo[pending] if len(pending) else np.zeros(0, dtype=np.int64)
         K_run *= 4
     for t in todo:
         K_used[t] = -1  # not determined within K_max primes
@@ -178,23 +182,40 @@ def exact_estimator(rs, method):
     return r3
 
 
-def rounding_floor(rs, method, u=Fraction(1, 2 ** 51)):
+def rounding_floor(rs, method, u=2.0 ** -51):
     """The estimator's relative change when each exact ratio moves by a
     relative u (4 units of 2^-53 by default): the error that computing the
     ratios in double precision alone can leave in the limit, however exact
     the walk. Aitken's estimator divides by a second difference of the
     ratios, so on partially converged walks this floor reaches 1e-10 and
-    beyond. None where the estimator has no exact value."""
+    beyond. None where the estimator has no exact value.
+
+    Worked in floating point from the exact differences D = r2 - r3 and
+    E = r1 - 2 r2 + r3 (exact, then rounded), so that the perturbed
+    estimate's change is formed from the small increments themselves:
+    dL = e3 r3 - ((2 D dD + dD^2) E - D^2 dE) / (E (E + dE)) with
+    dD = e2 r2 - e3 r3, dE = e1 r1 - 2 e2 r2 + e3 r3, e_i = +-u."""
     L = exact_estimator(rs, method)
     if L is None or L == 0:
         return None
-    worst = Fraction(0)
-    for signs in ((a, b, c) for a in (-1, 1) for b in (-1, 1) for c in (-1, 1)):
-        moved = [r * (1 + sg * u) for r, sg in zip(rs, signs)]
-        Lm = exact_estimator(moved, method)
-        if Lm is None:
-            return math.inf
-        worst = max(worst, abs(Lm - L) / abs(L))
+    r1, r2, r3 = rs
+    Lf = abs(float(L))
+    f1, f2, f3 = float(r1), float(r2), float(r3)
+    if method != 1 or r1 - 2 * r2 + r3 == 0:
+        return float(u * abs(f3) / Lf)
+    D, E = float(r2 - r3), float(r1 - 2 * r2 + r3)
+    worst = 0.0
+    for e1 in (-u, u):
+        for e2 in (-u, u):
+            for e3 in (-u, u):
+                dD = e2 * f2 - e3 * f3
+                dE = e1 * f1 - 2.0 * e2 * f2 + e3 * f3
+                if E + dE == 0.0:
+                    # the moved second difference vanishes: the estimate falls back to r3
+                    dL = (f3 * (1.0 + e3)) - float(L)
+                else:
+                    dL = e3 * f3 - ((2.0 * D * dD + dD * dD) * E - D * D * dE) / (E * (E + dE))
+                worst = max(worst, abs(dL) / Lf)
     return float(worst)
 
 

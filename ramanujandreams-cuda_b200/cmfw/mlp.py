@@ -93,6 +93,34 @@ class Mlp:
                  _ptr(d_scores), api._stream_handle(stream)))
         return d_scores[:n]
 
+    def score_indices(self, seed, d_idx, naxes, lo, hi, family, d_scores=None, stream=None):
+        """Scores of the candidates d_idx (int64 device tensor), one fused launch."""
+        torch = api._torch()
+        n = int(d_idx.numel())
+        if d_scores is None:
+            d_scores = torch.empty(max(n, 1), dtype=torch.float32, device="cuda")
+        check(lib().cmfw_mlp_score_indices(self.h, ctypes.c_uint64(seed), _ptr(d_idx), n, int(naxes), int(lo),
+                                           int(hi), int(family), _ptr(d_scores), api._stream_handle(stream)))
+        return d_scores[:n]
+
+
+def filter_candidates(desc, seed, first, n, lo, hi, start, N, h, steps=1, cap=None, stream=None):
+    """Indices (int64 device tensor, ascending) of candidates first ..
+    first+n-1 that pass the chunked walk's singularity filter; the others
+    are invalid walks."""
+    torch = api._torch()
+    cap = int(cap if cap is not None else max(1024, n // 256))
+    d_idx = torch.empty(max(cap, 1), dtype=torch.int64, device="cuda")
+    d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    st = (ctypes.c_double * 16)(*(list(start) + [0.0] * (16 - len(start))))
+    check(lib().cmfw_filter_candidates(ctypes.byref(desc), ctypes.c_uint64(seed), int(first), int(n), int(lo),
+                                       int(hi), st, int(N), int(h), int(steps), _ptr(d_idx), cap, _ptr(d_cnt),
+                                       api._stream_handle(stream)))
+    count = int(d_cnt.item())
+    if count > cap:
+        return filter_candidates(desc, seed, first, n, lo, hi, start, N, h, steps, 2 * count, stream)
+    return torch.sort(d_idx[:count])[0]
+
 
 def candidate_records(seed, d_idx, naxes, lo, hi, start, stream=None):
     """Device records of candidates d_idx (int64 tensor) of the seeded generator."""

@@ -2,24 +2,32 @@
 
 A delta search over a seeded candidate set (cmfw.mlp's generator:
 directions with components uniform in lo..hi over the family's axes, start
-at the zeta point) either walks every candidate (the plain exhaustive sweep,
-which stays the judge) or:
+at the zeta point) starts with the walk's own singularity filter
+(cmfw_filter_candidates: the position-only tests of the first lattice step,
+drawn in place, no records): every candidate that fails it is an invalid
+walk, and at a zeta start that is almost all of them. Then either
 
-1. walks a training set of candidates disjoint from the searched ones and
-   regresses their outcome with the tensor-core MLP (target: log1p-compressed
-   delta where the walk is valid and delta finite, VALID_NAN for valid walks
-   without a delta, FLOOR for invalid walks; valid rows weighted up);
-2. scores every searched candidate with the network;
-3. walks only the top-scoring candidates and keeps the best deltas;
-4. confirms the reported results against the exact rational walk.
+* the plain exhaustive sweep (the judge) walks every survivor, or
+* the proposal scores the survivors with the tensor-core MLP and walks only
+  the top `fraction` of them, keeping the best deltas.
 
-All walks, scoring and selection run on the GPU through the C ABI; GPU time
-is summed from CUDA events around each enqueued stage.
+The network is trained beforehand on walks of the survivors of a disjoint
+candidate range (target: log1p-compressed delta where the walk is valid and
+delta finite, VALID_NAN for valid walks without a delta, FLOOR for walks
+that fail later; the rare invalid survivors weighted to balance). Reported
+results are confirmed against the exact rational walk.
+
+Every walk is batch-invariant (CMFW_F_BATCH_INVARIANT): a candidate's
+delta is the same bits whether the sweep or the proposal walks it, so the
+proposal's finds are the sweep's own values. All filtering, walks, scoring
+and selection run on the GPU through the C ABI; GPU time is summed from
+CUDA events around each enqueued stage, per stage.
 """
 import numpy as np
 
 from . import api, exact
 from . import mlp as cm
+from ._lib import F_BATCH_INVARIANT
 from .mlp import FAMILY_INDEX
 
 FLOOR = -3.0  # target of invalid walks
@@ -53,33 +61,11 @@ class GpuClock:
         return False
 
 
-def _walk_range(desc, seed, first, n, naxes, lo, hi, start, N, h, variant, batch, clock):
-    """Walk candidates first .. first+n-1; returns (indices, delta, limit) of
-    the valid ones with a finite delta, and the number valid."""
-    torch = api._torch()
-    keep_i, keep_d, keep_l = [], [], []
-    n_valid = 0
-    for b in range(0, n, batch):
-        m = min(batch, n - b)
-        with clock:
-            idx = torch.arange(first + b, first + b + m, dtype=torch.int64, device="cuda")
-            recs = cm.candidate_records(seed, idx, naxes, lo, hi, start)
-            out = api.out_buffer(m)
-            api.launch_walk(variant, desc, recs, out, m, N, h)
-        res = api.records_from_device(out, m)
-        v = res["valid"] == 1
-        n_valid += int(v.sum())
-        ok = v & np.isfinite(res["delta"])
-        keep_i.append(np.nonzero(ok)[0] + first + b)
-        keep_d.append(res["delta"][ok])
-        keep_l.append(res["limit"][ok])
-    cat = (lambda xs, dt: np.concatenate(xs) if xs else np.zeros(0, dt))
-    return cat(keep_i, np.int64), cat(keep_d, np.float64), cat(keep_l, np.float64), n_valid
-
-
 def _walk_indices(desc, seed, idx_dev, naxes, lo, hi, start, N, h, variant, batch, clock):
-    torch = api._torch()
-    keep_i, keep_d = [], []
+    """Walk candidates idx_dev (int64 device tensor); returns (indices,
+    deltas, limits) of the valid ones with a finite delta, the number valid,
+    and every walked candidate's validity and delta (host arrays)."""
+    keep_i, keep_d, keep_l, all_v, all_d = [], [], [], [], []
     n_valid = 0
     n = int(idx_dev.numel())
     for b in range(0, n, batch):
@@ -88,15 +74,20 @@ def _walk_indices(desc, seed, idx_dev, naxes, lo, hi, start, N, h, variant, batc
         with clock:
             recs = cm.candidate_records(seed, sub, naxes, lo, hi, start)
             out = api.out_buffer(m)
-            api.launch_walk(variant, desc, recs, out, m, N, h)
+            api.launch_walk(variant, desc, recs, out, m, N, h, flags=F_BATCH_INVARIANT)
         res = api.records_from_device(out, m)
         v = res["valid"] == 1
         n_valid += int(v.sum())
         ok = v & np.isfinite(res["delta"])
-        keep_i.append(sub.cpu().numpy()[ok])
+        host = sub.cpu().numpy()
+        keep_i.append(host[ok])
         keep_d.append(res["delta"][ok])
+        keep_l.append(res["limit"][ok])
+        all_v.append(v)
+        all_d.append(res["delta"])
     cat = (lambda xs, dt: np.concatenate(xs) if xs else np.zeros(0, dt))
-    return cat(keep_i, np.int64), cat(keep_d, np.float64), n_valid
+    return (cat(keep_i, np.int64), cat(keep_d, np.float64), cat(keep_l, np.float64), n_valid,
+            cat(all_v, bool), cat(all_d, np.float64))
 
 
 def top_k(idx, delta, k):
@@ -118,44 +109,48 @@ class DeltaSearch:
         self.start = [1.0] * p + [2.0] * q
         self.family = FAMILY_INDEX[(p, q)]
 
+    def survivors(self, first, n, clock=None):
+        """Candidates first .. first+n-1 that pass the walk's singularity
+        filter (int64 device tensor, ascending)."""
+        clock = clock or GpuClock()
+        with clock:
+            out = cm.filter_candidates(self.desc, self.seed, first, n, self.lo, self.hi, self.start, self.N, self.h)
+        return out
+
     # -- the judge ------------------------------------------------------------
     def sweep(self, n, k=100):
-        """Walk candidates 0 .. n-1; returns (top-k indices, their deltas,
-        number valid, GPU ms)."""
-        clock = GpuClock()
-        idx, d, _, n_valid = _walk_range(self.desc, self.seed, 0, n, self.naxes, self.lo, self.hi, self.start, self.N,
-                                         self.h, self.variant, self.batch, clock)
+        """Filter candidates 0 .. n-1 and walk every survivor; returns
+        (top-k indices, their deltas, number valid, GPU ms, stage record)."""
+        c_filter, c_walk = GpuClock(), GpuClock()
+        surv = self.survivors(0, n, c_filter)
+        idx, d, _, n_valid, _, _ = _walk_indices(self.desc, self.seed, surv, self.naxes, self.lo, self.hi,
+                                                 self.start, self.N, self.h, self.variant, self.batch, c_walk)
         ti, td = top_k(idx, d, k)
-        return ti, td, n_valid, clock.ms
+        return ti, td, n_valid, c_filter.ms + c_walk.ms, {"filter_ms": c_filter.ms, "walk_ms": c_walk.ms,
+                                                          "survivors": int(surv.numel())}
 
     # -- training -------------------------------------------------------------
     def training_set(self, n, offset):
-        """Walk candidates offset .. offset+n-1 (disjoint from the searched
-        ones); returns device records, family ids, targets, weights and GPU ms."""
+        """Walk the survivors of candidates offset .. offset+n-1 (disjoint
+        from the searched ones); returns device records, family ids,
+        targets, weights and GPU ms."""
         torch = api._torch()
         clock = GpuClock()
-        targets = np.full(n, FLOOR, np.float32)
-        weights = np.ones(n, np.float32)
-        for b in range(0, n, self.batch):
-            m = min(self.batch, n - b)
-            with clock:
-                idx = torch.arange(offset + b, offset + b + m, dtype=torch.int64, device="cuda")
-                recs = cm.candidate_records(self.seed, idx, self.naxes, self.lo, self.hi, self.start)
-                out = api.out_buffer(m)
-                api.launch_walk(self.variant, self.desc, recs, out, m, self.N, self.h)
-            res = api.records_from_device(out, m)
-            valid = res["valid"] == 1
-            ok = valid & np.isfinite(res["delta"])
-            t = targets[b:b + m]
-            t[valid] = VALID_NAN
-            t[ok] = delta_target(res["delta"][ok])
-        # the rare valid rows carry as much total weight as the invalid ones
-        inf = targets > FLOOR
-        if inf.any():
-            weights[inf] = max(1.0, float((~inf).sum()) / float(inf.sum()))
-        idx = torch.arange(offset, offset + n, dtype=torch.int64, device="cuda")
-        recs = cm.candidate_records(self.seed, idx, self.naxes, self.lo, self.hi, self.start)
-        fam = torch.full((n,), self.family, dtype=torch.int32, device="cuda")
+        surv = self.survivors(offset, n, clock)
+        _, _, _, _, valid, delta = _walk_indices(self.desc, self.seed, surv, self.naxes, self.lo, self.hi,
+                                                 self.start, self.N, self.h, self.variant, self.batch, clock)
+        m = int(surv.numel())
+        targets = np.full(m, FLOOR, np.float32)
+        weights = np.ones(m, np.float32)
+        ok = valid & np.isfinite(delta)
+        targets[valid] = VALID_NAN
+        targets[ok] = delta_target(delta[ok])
+        # the invalid survivors carry as much total weight as the valid ones
+        bad = targets <= FLOOR
+        if bad.any() and (~bad).any():
+            weights[bad] = max(1.0, float((~bad).sum()) / float(bad.sum()))
+        recs = cm.candidate_records(self.seed, surv, self.naxes, self.lo, self.hi, self.start)
+        fam = torch.full((m,), self.family, dtype=torch.int32, device="cuda")
         return recs, fam, torch.from_numpy(targets).cuda(), torch.from_numpy(weights).cuda(), clock.ms
 
     def train(self, net, data, epochs=3, batch=8192, lr=1e-3, seed=0):
@@ -163,6 +158,7 @@ class DeltaSearch:
         torch = api._torch()
         recs, fam, y, w = data
         n = recs.shape[0]
+        batch = min(batch, max(128, n // 4 // 128 * 128))
         g = torch.Generator(device="cpu").manual_seed(seed)
         clock = GpuClock()
         for _ in range(epochs):
@@ -176,22 +172,30 @@ class DeltaSearch:
         return clock.ms
 
     # -- the proposal ---------------------------------------------------------
-    def propose(self, net, n, fraction, k=100):
-        """Score candidates 0 .. n-1, walk the top `fraction`, return (top-k
-        indices, deltas, number walked, number valid, GPU ms by stage)."""
+    def propose(self, net, n, fraction, k=100, rank="network", rng_seed=0):
+        """Filter candidates 0 .. n-1, score the survivors, walk the top
+        `fraction` of them; returns (top-k indices, deltas, number walked,
+        number valid, GPU ms by stage). rank="random" walks the same number
+        of survivors chosen without the network (the method without it)."""
         torch = api._torch()
-        scores = torch.empty(n, dtype=torch.float32, device="cuda")
-        c_score, c_select, c_walk = GpuClock(), GpuClock(), GpuClock()
-        with c_score:
-            net.score_candidates(self.seed, 0, n, self.naxes, self.lo, self.hi, self.family, scores)
-        n_walk = max(1, int(round(fraction * n)))
-        with c_select:
-            sel = cm.select_top(scores, n_walk)
-        idx, d, n_valid = _walk_indices(self.desc, self.seed, sel, self.naxes, self.lo, self.hi, self.start, self.N,
-                                        self.h, self.variant, self.batch, c_walk)
+        c_filter, c_score, c_select, c_walk = GpuClock(), GpuClock(), GpuClock(), GpuClock()
+        surv = self.survivors(0, n, c_filter)
+        m = int(surv.numel())
+        n_walk = min(m, max(1, int(round(fraction * m))))
+        if rank == "random":
+            g = torch.Generator(device="cpu").manual_seed(rng_seed)
+            sel = surv[torch.randperm(m, generator=g)[:n_walk].cuda()]
+        else:
+            with c_score:
+                scores = net.score_indices(self.seed, surv, self.naxes, self.lo, self.hi, self.family)
+            with c_select:
+                sel = surv[cm.select_top(scores, n_walk)] if m else surv
+        idx, d, _, n_valid, _, _ = _walk_indices(self.desc, self.seed, sel, self.naxes, self.lo, self.hi,
+                                                 self.start, self.N, self.h, self.variant, self.batch, c_walk)
         ti, td = top_k(idx, d, k)
         net.status()
-        return ti, td, int(sel.numel()), n_valid, {"score": c_score.ms, "select": c_select.ms, "walk": c_walk.ms}
+        return ti, td, int(sel.numel()), n_valid, {"filter": c_filter.ms, "score": c_score.ms,
+                                                   "select": c_select.ms, "walk": c_walk.ms, "survivors": m}
 
     def confirm(self, indices, limits=None, rtol=1e-10, detail=False):
         """Exact check of the reported trajectories' f64 limits (the walk

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "cmfw.h"
+#include "candidates.cuh"
 #include "cmfw_internal.cuh"
 #include "tc_sm100.cuh"
 
@@ -206,21 +207,6 @@ __global__ void features_kernel(const cmfw_traj_in *in, const int *family, int n
     X[i] = __float2bfloat16_rn(v);
 }
 
-// Candidate directions from a counter-based generator (splitmix64 of
-// seed + index), components lo + (draw mod (hi - lo + 1)) for naxes axes:
-// one 64-bit draw per 4 components (16 bits each).
-__host__ __device__ inline uint64_t splitmix64(uint64_t x) {
-    x += 0x9E3779B97F4A7C15ull;
-    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
-    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
-    return x ^ (x >> 31);
-}
-
-__device__ __forceinline__ int candidate_component(uint64_t seed, long long idx, int a, int lo, int span) {
-    const uint64_t w = splitmix64(seed ^ ((uint64_t)idx * 4ull + (uint64_t)(a >> 2)) * 0xD1B54A32D192ED03ull);
-    return lo + (int)(((w >> (16 * (a & 3))) & 0xFFFFull) % (uint64_t)span);
-}
-
 __global__ void candidate_features_kernel(uint64_t seed, long long first, int n, int n_pad, int naxes, int lo,
                                           int hi, int family, __nv_bfloat16 *X) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -396,6 +382,7 @@ struct FusedArgs {
     const float *w4, *b4;
     uint64_t seed;
     long long first, n;
+    const long long *idx;  // optional: score candidates idx[0..n) instead of first .. first+n-1
     int naxes, lo, hi, family;
     float *score;
     int *err;
@@ -484,10 +471,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256) mlp_score_fused
 #pragma unroll
             for (int f = 0; f < 24; ++f) v[f] = 0.0f;
             if (cand < a.n) {
-                const long long idx = a.first + cand;
+                const long long idx = a.idx ? __ldg(a.idx + cand) : a.first + cand;
 #pragma unroll
                 for (int w = 0; w < 4; ++w) {
-                    const uint64_t d = splitmix64(a.seed ^ ((uint64_t)idx * 4ull + (uint64_t)w) * 0xD1B54A32D192ED03ull);
+                    const uint64_t d = candidate_draw(a.seed, idx, w);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int f = 4 * w + q;
@@ -908,8 +895,8 @@ cmfw_status cmfw_mlp_score_candidates(cmfw_mlp *M, uint64_t seed, long long firs
     return CMFW_OK;
 }
 
-cmfw_status cmfw_mlp_score_candidates_fused(cmfw_mlp *M, uint64_t seed, long long first, long long n, int naxes,
-                                            int lo, int hi, int family, float *d_scores, void *stream) {
+static cmfw_status score_fused(cmfw_mlp *M, uint64_t seed, long long first, const long long *d_idx, long long n,
+                               int naxes, int lo, int hi, int family, float *d_scores, void *stream) {
     if (!M || !d_scores) return record_error(CMFW_EINVAL, "NULL argument");
     if (n < 0 || naxes < 1 || naxes > 15 || hi < lo || family < 0 || family > 4)
         return record_error(CMFW_EINVAL, "candidate range out of bounds");
@@ -928,6 +915,7 @@ cmfw_status cmfw_mlp_score_candidates_fused(cmfw_mlp *M, uint64_t seed, long lon
     a.seed = seed;
     a.first = first;
     a.n = n;
+    a.idx = d_idx;
     a.naxes = naxes;
     a.lo = lo;
     a.hi = hi;
@@ -954,6 +942,17 @@ cmfw_status cmfw_mlp_score_candidates_fused(cmfw_mlp *M, uint64_t seed, long lon
     e = cudaLaunchKernelEx(&cfg, mlp_score_fused_kernel, a);
     if (e == cudaSuccess) e = cudaGetLastError();
     return e == cudaSuccess ? CMFW_OK : cuda_fail(e, "fused scoring launch");
+}
+
+cmfw_status cmfw_mlp_score_candidates_fused(cmfw_mlp *M, uint64_t seed, long long first, long long n, int naxes,
+                                            int lo, int hi, int family, float *d_scores, void *stream) {
+    return score_fused(M, seed, first, nullptr, n, naxes, lo, hi, family, d_scores, stream);
+}
+
+cmfw_status cmfw_mlp_score_indices(cmfw_mlp *M, uint64_t seed, const long long *d_idx, long long n, int naxes,
+                                   int lo, int hi, int family, float *d_scores, void *stream) {
+    if (n > 0 && !d_idx) return record_error(CMFW_EINVAL, "NULL index list");
+    return score_fused(M, seed, 0, d_idx, n, naxes, lo, hi, family, d_scores, stream);
 }
 
 cmfw_status cmfw_candidate_records(uint64_t seed, const long long *d_idx, int n, int naxes, int lo, int hi,

@@ -503,7 +503,10 @@ __global__ void __launch_bounds__(chunk_threads(DIM), 1) walk_chunk_kernel(Chunk
     if (tid < 32) {
         const int count = *C.count;
         const int Gr = min(min((int)gridDim.x, C.nslots), min(C.part_budget, kMaxPartBudget));
-        const bool bal = count > 0 && count <= Gr;
+        // CMFW_F_BATCH_INVARIANT: one CTA per survivor whatever the batch, so
+        // a trajectory's run geometry (and every rounding) is the same in
+        // every batch
+        const bool bal = count > 0 && count <= Gr && !(W.flags & CMFW_F_BATCH_INVARIANT);
         int b0 = -1, part0 = 0, np0 = 1, first0 = 0;
         if (bal) {
             int w[kLaneItems];

@@ -35,6 +35,7 @@
 // trajectory, a plain grid of 256-thread CTAs.
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "cmfw.h"
@@ -464,6 +465,22 @@ cmfw_mixed_tuning default_tuning(int n_descs) {
     return t;
 }
 
+// Candidate c of the autotuner's whole-batch stage: -2 the plain 256-thread
+// grid everywhere (the fixed baseline), -1 the per-family choices, 0..8
+// tile c (block blocks[c / 3], grab grabs[c % 3]) for every family.
+cmfw_mixed_tuning joint_candidate(const cmfw_mixed_tuning &per_family, int c, int n_descs, const int *blocks,
+                                  const int *grabs) {
+    cmfw_mixed_tuning t = per_family;
+    if (c == -2) t.persistent = 0;
+    if (c >= 0)
+        for (int f = 0; f < n_descs; ++f) {
+            t.tile[f].block_size = blocks[c / 3];
+            t.tile[f].grab = grabs[c % 3];
+            t.tile[f].ctas_per_sm = 0;
+        }
+    return t;
+}
+
 }  // namespace
 
 struct cmfw_mixed_graph {
@@ -589,21 +606,37 @@ cmfw_status cmfw_mixed_autotune(const cmfw_desc *descs, int n_descs, const cmfw_
         Mj.begin = d_sbegin;
         Mj.next = d_snext;
         const cmfw_mixed_tuning per_family = *out;
-        float best = 1e30f;
+        std::vector<std::pair<float, int>> timed;  // (sample ms, candidate)
         for (int c = -2; c < 9 && e == cudaSuccess; ++c) {
-            cmfw_mixed_tuning t = per_family;
-            if (c == -2) t.persistent = 0;  // the plain 256-thread grid everywhere
-            if (c >= 0)
-                for (int f = 0; f < n_descs; ++f) {
-                    t.tile[f].block_size = blocks[c / 3];
-                    t.tile[f].grab = grabs[c % 3];
-                    t.tile[f].ctas_per_sm = 0;
-                }
+            const cmfw_mixed_tuning t = joint_candidate(per_family, c, n_descs, blocks, grabs);
             float ms = 0.f;
             for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {  // warm-up, then timed
                 e = cudaMemsetAsync(d_snext, 0, sizeof(int) * CMFW_MAX_MIXED_DESCS, s);
                 if (e == cudaSuccess) e = cudaEventRecord(a, s);
                 if (e == cudaSuccess) e = enqueue_families_forked(Mj, L, variant, t, s);
+                if (e == cudaSuccess) e = cudaEventRecord(b, s);
+                if (e == cudaSuccess) e = cudaEventSynchronize(b);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+            }
+            if (e == cudaSuccess) timed.push_back({ms, c});
+        }
+        // A sample ranks the candidates but can misjudge the whole batch's
+        // tails: the fastest three on the sample and the fixed baseline (the
+        // plain 256-thread grid, c = -2) are timed on the whole batch, and
+        // the fastest of those is kept -- so the tuning never loses to the
+        // baseline by more than the timing noise.
+        std::sort(timed.begin(), timed.end());
+        std::vector<int> finalists;
+        for (size_t i = 0; i < timed.size() && finalists.size() < 3; ++i) finalists.push_back(timed[i].second);
+        if (std::find(finalists.begin(), finalists.end(), -2) == finalists.end()) finalists.push_back(-2);
+        float best = 1e30f;
+        for (int c : finalists) {
+            if (e != cudaSuccess) break;
+            const cmfw_mixed_tuning t = joint_candidate(per_family, c, n_descs, blocks, grabs);
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+                e = cudaEventRecord(a, s);
+                if (e == cudaSuccess) e = enqueue_mixed(M, L, variant, t, s);
                 if (e == cudaSuccess) e = cudaEventRecord(b, s);
                 if (e == cudaSuccess) e = cudaEventSynchronize(b);
                 if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);

@@ -125,16 +125,21 @@ def test_cfg1_limit_starts_match_oracle(cuda):
 def test_cfg3_8f7_zeta_rns(cuda, N, K):
     """8F7 at the zeta point, directions 1^15 + U{0..2}^15, compat RNS with
     K moduli: validity equal to the oracle (under the reference's path order
-    the first y+ step of a zeta start is singular, so every trajectory is
-    invalid), and -- so that the residues are compared on real walks --
-    8F7 z = 1/2 walks of the reference's inputs at the same N and K, whose
-    limits, p and q agree with the oracle bit for bit."""
+    the first y+ step of a zeta start is singular unless an x step comes
+    first, so most trajectories are invalid) and the valid ones' limit, p
+    and q bit for bit; then 8F7 z = 1/2 walks of the reference's inputs at
+    the same N and K with their residue traces."""
     recs = wl.zeta_directions(8, 7, 2000, 20261203, lo=0, hi=2, offset=1)
     desc = cmfw.make_desc(8, 7, 1.0)
     g = cmfw.walk("rns", desc, recs, N, 50, n_primes=K)
-    o = oracle.walk("rns", 8, 7, 1.0, N, 50, recs[:200], n_primes=K, fused=True)
-    np.testing.assert_array_equal(g["valid"][:200], o["valid"])
-    assert (g["valid"] == 0).all()
+    # the oracle on the rows the GPU walks validly and on 100 others
+    pick = np.concatenate([np.nonzero(g["valid"] == 1)[0][:40], np.arange(100)])
+    o = oracle.walk("rns", 8, 7, 1.0, N, 50, recs[pick], n_primes=K, fused=True)
+    np.testing.assert_array_equal(g["valid"][pick], o["valid"])
+    assert (g["valid"] == 1).mean() < 0.1  # the first y+ step of a zeta start is singular for most
+    mv = o["valid"] == 1
+    for k in ("limit", "p", "q"):
+        assert np.array_equal(g[k][pick][mv], o[k][mv], equal_nan=True), k
     live = oracle.make_inputs(8, 7, 30, 0, False)[:8]
     desc = cmfw.make_desc(8, 7, 0.5)
     g = cmfw.walk("rns", desc, live, N, 50, n_primes=K)

@@ -63,27 +63,37 @@ def _limit_parity(desc, recs, g, src, o, N, h, rtol=1e-9):
         g_ok = np.abs(g["limit"][far] - L) <= rtol * np.abs(L)
         o_ok = np.abs(o["limit"][far] - L) <= rtol * np.abs(L)
     undefined = np.isnan(L) | np.isinf(L)
+    # an estimator whose rounding floor (the change of the estimate when the
+    # exact ratios move by 4 ulps) is not far below rtol decides by rounding
+    # which build lands within rtol
+    noisy = ~(v["floor"] <= rtol / 100)
     # a row fails only where the reference's own value is exact to rtol and
     # the GPU's is not; elsewhere both are rounding noise of an
     # ill-conditioned walk (or the estimator has no exact value)
-    bad = far[~(g_ok | undefined | ~o_ok)]
+    bad = far[~(g_ok | undefined | noisy | ~o_ok)]
     assert len(bad) == 0, [(int(t), float(g["limit"][t]), float(o["limit"][t])) for t in bad[:5]]
-    assert g_ok.sum() >= o_ok.sum() - 1
+    assert g_ok.sum() >= o_ok.sum() - 1 - len(far) // 100
     return len(far)
 
 
 def _tail_parity(g, o, same_tol, tol, min_rows=0, lim_tol=1e-9):
     """precision and delta (cmf_pfq.cuh:476-552) against the oracle, on the
     valid rows whose limit the two agree on within lim_tol (the same
-    estimator). Both fields
-    take logs of differences of nearly converged ratios, so:
-      * which rows are NaN or infinite must agree exactly;
-      * values are compared where they are well conditioned -- the ratios at
-        N and N-h differ by more than 1e-6 relative (the oracle's precision
-        says how much), so a relative error e of the walk moves precision
-        by about e * 1e6 / ln 10 digits -- and where the GPU's p/q agree with
-        the oracle's within same_tol: there, within tol (precision, digits)
-        and tol * max(1, |delta|) (delta) on at least 95% of the rows.
+    estimator). Both fields take logs of differences of nearly converged
+    ratios, so:
+      * which rows are NaN must agree exactly (NaN comes from the structure
+        of the walk: a vanishing q, log q <= 0, no finite limit);
+      * rows converged to the rounding level (precision 12 or more, or
+        infinite -- the ratios at N and N-h equal to the last bit -- on
+        either side) carry rounding noise in both fields and are compared
+        no further;
+      * on the other rows infinities must agree, and the values are
+        compared where well conditioned -- the ratios at N and N-h differ by
+        more than 1e-6 relative, so a relative error e of the walk moves
+        precision by about e * 1e6 / ln 10 digits -- and where the GPU's p/q
+        agree with the oracle's within same_tol: there, within tol
+        (precision, digits) and tol * max(1, |delta|) (delta) on at least 95%
+        of the rows.
     Returns the number of value-compared rows."""
     m = (g["valid"] == 1) & (o["valid"] == 1)
     with np.errstate(invalid="ignore"):
@@ -92,11 +102,15 @@ def _tail_parity(g, o, same_tol, tol, min_rows=0, lim_tol=1e-9):
     m &= lim_same
     for k in ("precision", "delta"):
         assert np.array_equal(np.isnan(g[k][m]), np.isnan(o[k][m])), k
-        assert np.array_equal(np.isinf(g[k][m]), np.isinf(o[k][m])), k
+    with np.errstate(invalid="ignore"):
+        converged = (np.nan_to_num(g["precision"], nan=0.0) >= 12.0) | (np.nan_to_num(o["precision"], nan=0.0) >= 12.0)
+    live = m & ~converged
+    for k in ("precision", "delta"):
+        assert np.array_equal(np.isinf(g[k][live]), np.isinf(o[k][live])), k
     with np.errstate(invalid="ignore", divide="ignore"):
         rel_pq = np.abs(g["p"] / g["q"] - o["p"] / o["q"]) / np.abs(o["p"] / o["q"])
         scale = np.log10(np.maximum(np.abs(o["limit"]), 1e-300))
-        cond = m & np.isfinite(o["precision"]) & (o["precision"] < 6.0 - scale) & (rel_pq <= same_tol)
+        cond = live & np.isfinite(o["precision"]) & (o["precision"] < 6.0 - scale) & (rel_pq <= same_tol)
     cond &= np.isfinite(o["delta"])
     n = int(cond.sum())
     assert n >= min_rows, n
