@@ -642,9 +642,9 @@ def main_proposal(args):
     n_search, n_train = int(args.search_n), int(args.train_n)
     S = prop.DeltaSearch(8, 7, 0, 4, N, H, "df64", SEED)
     S.sweep(min(1 << 22, n_search))  # warm (allocations, kernel set-up)
+    S.survivors(0, n_search)  # and the filter at full size
     sw_i, sw_d, sw_valid, sw_ms, sw_st = S.sweep(n_search)
     data = S.training_set(n_train, 1 << 40)
-    y = data[2].cpu().numpy()
     net = cm.Mlp(1 << 16, seed=1)
     train_ms = S.train(net, data[:4], epochs=args.epochs)
     S.propose(net, min(1 << 22, n_search), args.fraction)  # warm
@@ -664,8 +664,8 @@ def main_proposal(args):
                   "survivors": sw_st["survivors"], "n_valid": sw_valid,
                   "top100_min_delta": float(sw_d[-1]) if len(sw_d) else None,
                   "top100_confirmed_exact": confirmed},
-        "training": {"walk_gpu_ms": data[4], "train_gpu_ms": train_ms, "n_walked": int(len(y)),
-                     "n_valid": int((y > prop.FLOOR).sum()), "n_finite_delta": int((y > prop.VALID_NAN).sum())},
+        "training": {"walk_gpu_ms": data[4], "train_gpu_ms": train_ms, **S.train_stats,
+                     "target": f"top {prop.TOP_Q:.0%} of the training walks' finite deltas (weighted 0/1)"},
         "proposal": {"gpu_ms": prop_ms, "stages_ms": {k: v for k, v in st.items() if k != "survivors"},
                      "n_walked": n_walk, "n_valid_walked": p_valid,
                      "found": len(set(p_i.tolist()) & set(sw_i.tolist()))},

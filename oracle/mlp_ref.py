@@ -35,14 +35,32 @@ def flatten(parts):
     return np.concatenate([np.asarray(p).reshape(-1) for p in parts])
 
 
+FAMILY_P = [3, 4, 5, 6, 8]
+
+
 def features(dirs, family):
-    """X [n x 64]: dir[0..14] / 4, one-hot(family) at 15..19, zeros."""
+    """X [n x 64], as the device's direction_features (csrc/candidates.cuh):
+    for the x components (the family's first p axes) and the y components
+    (the next q = p - 1), how many have |d| = 0, 1, 2, 3 and >= 4, over p
+    (columns 0..4) and over q (5..9); the negative ones over p and q (10,
+    11); one-hot(family) at 15..19; zeros elsewhere; rounded to BF16."""
     dirs = np.asarray(dirs)
+    family = np.asarray(family)
     n = len(dirs)
     X = np.zeros((n, 64), np.float32)
-    X[:, :15] = 0.25 * dirs[:, :15]
-    X[np.arange(n), 15 + np.asarray(family)] = 1.0
-    return X
+    for t in range(n):
+        p = FAMILY_P[int(family[t])]
+        q = p - 1
+        d = dirs[t, :p + q].astype(np.int64)
+        m = np.minimum(np.abs(d), 4)
+        ip, iq = np.float32(1.0) / np.float32(p), np.float32(1.0) / np.float32(q)
+        for k in range(5):
+            X[t, k] = np.float32((m[:p] == k).sum()) * ip
+            X[t, 5 + k] = np.float32((m[p:] == k).sum()) * iq
+        X[t, 10] = np.float32((d[:p] < 0).sum()) * ip
+        X[t, 11] = np.float32((d[p:] < 0).sum()) * iq
+        X[t, 15 + int(family[t])] = 1.0
+    return to_bf16(X)  # the device holds features in BF16
 
 
 def forward(params, X, bf16=True):

@@ -204,6 +204,8 @@ def rounding_floor(rs, method, u=2.0 ** -51):
     if method != 1 or r1 - 2 * r2 + r3 == 0:
         return float(u * abs(f3) / Lf)
     D, E = float(r2 - r3), float(r1 - 2 * r2 + r3)
+    if E == 0.0 or not math.isfinite(E) or not math.isfinite(D):
+        return math.inf  # the second difference is below the double range: no usable floor
     worst = 0.0
     for e1 in (-u, u):
         for e2 in (-u, u):

@@ -12,10 +12,15 @@ walk, and at a zeta start that is almost all of them. Then either
   the top `fraction` of them, keeping the best deltas.
 
 The network is trained beforehand on walks of the survivors of a disjoint
-candidate range (target: log1p-compressed delta where the walk is valid and
-delta finite, VALID_NAN for valid walks without a delta, FLOOR for walks
-that fail later; the rare invalid survivors weighted to balance). Reported
-results are confirmed against the exact rational walk.
+candidate range. Its target is whether a survivor's delta is among the top
+TOP_Q of the training walks' finite deltas (1 or 0, the rare positives
+weighted to balance the rest), so that its output ranks survivors by how
+likely they are to hold one of the search's best deltas; its features
+(direction_features in csrc/candidates.cuh) count the x and y components
+by magnitude, which the walk at the symmetric zeta start depends on.
+Regressing the delta itself ranked the top no better than chance: deltas
+span five orders of magnitude and the bulk of the loss is elsewhere.
+Reported results are confirmed against the exact rational walk.
 
 Every walk is batch-invariant (CMFW_F_BATCH_INVARIANT): a candidate's
 delta is the same bits whether the sweep or the proposal walks it, so the
@@ -30,15 +35,24 @@ from . import mlp as cm
 from ._lib import F_BATCH_INVARIANT
 from .mlp import FAMILY_INDEX
 
-FLOOR = -3.0  # target of invalid walks
-VALID_NAN = -2.0  # target of valid walks whose delta is undefined
+TOP_Q = 0.01  # training positives: the top 1% of the training walks' finite deltas
 
 
-def delta_target(delta):
-    """Regression target of a finite delta: sign-preserving log1p, so that
-    the rare huge deltas (exactly rational limits) do not dominate."""
-    d = np.asarray(delta, np.float64)
-    return (np.sign(d) * np.log1p(np.abs(d))).astype(np.float32)
+def top_target(valid, delta, top_q=TOP_Q):
+    """Training target and weights from walk outcomes: 1 where the walk is
+    valid and its delta finite and at least the (1 - top_q) quantile of the
+    finite deltas, else 0; positives weighted so that both classes carry
+    the same total weight. Returns (targets, weights, threshold)."""
+    valid = np.asarray(valid, bool)
+    delta = np.asarray(delta, np.float64)
+    fin = valid & np.isfinite(delta)
+    thr = float(np.quantile(delta[fin], 1.0 - top_q)) if fin.any() else np.inf
+    pos = fin & (delta >= thr)
+    t = pos.astype(np.float32)
+    w = np.ones(len(t), np.float32)
+    if pos.any() and (~pos).any():
+        w[pos] = float((~pos).sum()) / float(pos.sum())
+    return t, w, thr
 
 
 class GpuClock:
@@ -140,20 +154,15 @@ class DeltaSearch:
         _, _, _, _, valid, delta = _walk_indices(self.desc, self.seed, surv, self.naxes, self.lo, self.hi,
                                                  self.start, self.N, self.h, self.variant, self.batch, clock)
         m = int(surv.numel())
-        targets = np.full(m, FLOOR, np.float32)
-        weights = np.ones(m, np.float32)
-        ok = valid & np.isfinite(delta)
-        targets[valid] = VALID_NAN
-        targets[ok] = delta_target(delta[ok])
-        # the invalid survivors carry as much total weight as the valid ones
-        bad = targets <= FLOOR
-        if bad.any() and (~bad).any():
-            weights[bad] = max(1.0, float((~bad).sum()) / float(bad.sum()))
+        targets, weights, thr = top_target(valid, delta)
+        self.train_stats = {"walked": m, "valid": int(valid.sum()),
+                            "finite_delta": int((valid & np.isfinite(delta)).sum()),
+                            "positives": int(targets.sum()), "threshold": thr}
         recs = cm.candidate_records(self.seed, surv, self.naxes, self.lo, self.hi, self.start)
         fam = torch.full((m,), self.family, dtype=torch.int32, device="cuda")
         return recs, fam, torch.from_numpy(targets).cuda(), torch.from_numpy(weights).cuda(), clock.ms
 
-    def train(self, net, data, epochs=3, batch=8192, lr=1e-3, seed=0):
+    def train(self, net, data, epochs=30, batch=2048, lr=1e-3, seed=0):
         """Adam epochs over the training set in shuffled mini-batches; returns GPU ms."""
         torch = api._torch()
         recs, fam, y, w = data

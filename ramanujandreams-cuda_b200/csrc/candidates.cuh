@@ -27,4 +27,40 @@ __host__ __device__ inline int candidate_component(uint64_t seed, long long idx,
     return lo + (int)(((w >> (16 * (a & 3))) & 0xFFFFull) % (uint64_t)span);
 }
 
+// Network features of a direction d[0..naxes) of family `family` (0..4 =
+// 3F2, 4F3, 5F4, 6F5, 8F7; the first p axes are x-axes, the rest y-axes):
+// how many x components have |d| = 0, 1, 2, 3 and >= 4, over p (slots
+// 0..4), the same for the y components over q (5..9), the negative x and y
+// components over p and q (10, 11), zeros (12..14), and the family one-hot
+// (15..19). At a symmetric start (the zeta point: all x equal, all y
+// equal) the walk depends on a direction mostly through these counts, and
+// directions that differ only by permuting x or y components get the same
+// features.
+__host__ __device__ inline int family_p(int family) {
+    return family == 0 ? 3 : family == 1 ? 4 : family == 2 ? 5 : family == 3 ? 6 : 8;
+}
+template <class GET>
+__host__ __device__ inline void direction_features(GET comp, int naxes, int family, float *f /* 20 */) {
+    for (int k = 0; k < 20; ++k) f[k] = 0.0f;
+    int p = family_p(family);
+    if (p > naxes) p = naxes;
+    const int q = naxes - p;
+    for (int a = 0; a < naxes && a < 15; ++a) {
+        const int v = comp(a);
+        const int m = v < 0 ? -v : v;
+        const int bin = m < 4 ? m : 4;
+        const bool x = a < p;
+        f[(x ? 0 : 5) + bin] += 1.0f;
+        if (v < 0) f[x ? 10 : 11] += 1.0f;
+    }
+    const float ip = p > 0 ? 1.0f / (float)p : 0.0f, iq = q > 0 ? 1.0f / (float)q : 0.0f;
+    for (int k = 0; k < 5; ++k) {
+        f[k] *= ip;
+        f[5 + k] *= iq;
+    }
+    f[10] *= ip;
+    f[11] *= iq;
+    if (family >= 0 && family < 5) f[15 + family] = 1.0f;
+}
+
 }  // namespace cmfw

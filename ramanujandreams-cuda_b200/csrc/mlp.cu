@@ -14,8 +14,9 @@
 // dW = dZ^T X (A = dZ^T, B = X^T, both transposed by transpose_bf16_kernel).
 // The 256 -> 1 head, the loss, bias gradients and Adam are CUDA-core kernels.
 //
-// Inputs: features(t) = (dir[0..14] / 4, one-hot(family) over 5, zeros) as
-// 64 BF16 values. Parameters are FP32 masters with BF16 copies for the
+// Inputs: features(t) = direction_features (candidates.cuh: counts of the
+// x and y components by magnitude, signs, one-hot(family) over 5) padded
+// with zeros to 64 BF16 values. Parameters are FP32 masters with BF16 copies for the
 // tensor cores (W and W^T).
 #include <cstdio>
 #include <cstring>
@@ -194,15 +195,21 @@ static cudaError_t gemm(const GemmArgs &g, int epi, cudaStream_t s) {
 
 // ---- CUDA-core kernels ------------------------------------------------------
 
-// Features of n trajectories into X [n_pad x 64] bf16 (rows >= n zero).
+// Features (direction_features) of n trajectories into X [n_pad x 64] bf16
+// (rows >= n zero). The trajectory's family is d_family[t]; its axes are
+// the family's p + q.
 __global__ void features_kernel(const cmfw_traj_in *in, const int *family, int n, int n_pad, __nv_bfloat16 *X) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_pad * kIn) return;
     const int t = i / kIn, c = i % kIn;
     float v = 0.0f;
-    if (t < n) {
-        if (c < 15) v = 0.25f * (float)in[t].dir[c];
-        else if (c < 20) v = (family[t] == c - 15) ? 1.0f : 0.0f;
+    if (t < n && c < 20) {
+        const int fam = family[t];
+        const int p = family_p(fam);
+        const cmfw_traj_in &r = in[t];
+        float f[20];
+        direction_features([&](int a) { return r.dir[a]; }, p + (p - 1), fam, f);
+        v = f[c];
     }
     X[i] = __float2bfloat16_rn(v);
 }
@@ -213,9 +220,11 @@ __global__ void candidate_features_kernel(uint64_t seed, long long first, int n,
     if (i >= n_pad * kIn) return;
     const int t = i / kIn, c = i % kIn;
     float v = 0.0f;
-    if (t < n) {
-        if (c < naxes && c < 15) v = 0.25f * (float)candidate_component(seed, first + t, c, lo, hi - lo + 1);
-        else if (c >= 15 && c < 20) v = (family == c - 15) ? 1.0f : 0.0f;
+    if (t < n && c < 20) {
+        float f[20];
+        direction_features([&](int a) { return candidate_component(seed, first + t, a, lo, hi - lo + 1); }, naxes,
+                           family, f);
+        v = f[c];
     }
     X[i] = __float2bfloat16_rn(v);
 }
@@ -472,17 +481,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256) mlp_score_fused
             for (int f = 0; f < 24; ++f) v[f] = 0.0f;
             if (cand < a.n) {
                 const long long idx = a.idx ? __ldg(a.idx + cand) : a.first + cand;
+                int comp[16];
 #pragma unroll
                 for (int w = 0; w < 4; ++w) {
                     const uint64_t d = candidate_draw(a.seed, idx, w);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int f = 4 * w + q;
-                        if (f < 15 && f < a.naxes)
-                            v[f] = 0.25f * (float)(a.lo + (int)((uint32_t)((d >> (16 * q)) & 0xFFFFull) % (uint32_t)span));
-                    }
+                    for (int q = 0; q < 4; ++q)
+                        comp[4 * w + q] = a.lo + (int)((uint32_t)((d >> (16 * q)) & 0xFFFFull) % (uint32_t)span);
                 }
-                if (a.family >= 0 && a.family < 5) v[15 + a.family] = 1.0f;
+                direction_features([&](int k) { return comp[k]; }, a.naxes, a.family, v);
             }
 #pragma unroll
             for (int c = 0; c < 3; ++c) *(uint4 *)(act + tc::tile_offset(row, 8 * c, kIn)) = pack8(v + 8 * c);

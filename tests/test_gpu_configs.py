@@ -102,7 +102,7 @@ def test_valid_directions_are_valid_in_the_oracle(cuda):
 def test_cfg1_limit_starts_match_oracle(cuda):
     """3F2, z = 1/2, 10,000 starts U{1..10}, direction 1^5, N = 1000, h = 50:
     the CPU-baseline configuration, validity row for row and the limits."""
-    from test_gpu_walk import _close_fraction, _limit_parity
+    from test_gpu_walk import _exact_pq_parity, _limit_parity
     recs = wl.limit_starts(3, 2, 10000, 20261203)
     desc = cmfw.make_desc(3, 2, 0.5)
     g, src = cmfw.walk("f64", desc, recs, 1000, 50, with_limit_src=True)
@@ -116,8 +116,7 @@ def test_cfg1_limit_starts_match_oracle(cuda):
     gs, os_ = g.copy(), o.copy()
     gs["valid"][~sub] = 0
     _limit_parity(desc, recs, gs, src, os_, 1000, 50)
-    for k in ("p", "q", "log_scale"):
-        _close_fraction(g[k][m], o[k][m], 1e-9, k)
+    _exact_pq_parity(desc, recs, g, o, sub)
 
 
 @pytest.mark.parametrize("N", [1000, 4000])

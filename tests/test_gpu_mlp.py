@@ -34,16 +34,18 @@ def test_forward_and_gradients_match_reference(cuda):
     X = mlp_ref.features(recs["dir"], fam)
     s_ref, _ = mlp_ref.forward(params, X)
     s = m.forward(d_in, d_fam, n).cpu().numpy()
-    assert _rel(s, s_ref) < 1e-2, _rel(s, s_ref)
+    # the reference repeats the device's BF16 roundings; what remains is the
+    # FP32 accumulation order (measured: forward <= 1e-4, gradients <= 4e-4)
+    assert _rel(s, s_ref) < 1e-3, _rel(s, s_ref)
     rng = np.random.default_rng(2)
     y = rng.normal(0, 1, n).astype(np.float32)
     w = rng.uniform(0.5, 2.0, n).astype(np.float32)
     g, loss = m.gradients(d_in, d_fam, torch.from_numpy(y).cuda(), torch.from_numpy(w).cuda(), n, float(w.sum()))
     loss_ref, g_ref = mlp_ref.gradients(params, X, y, w, float(w.sum()))
-    assert abs(loss - loss_ref) <= 1e-2 * abs(loss_ref)
+    assert abs(loss - loss_ref) <= 1e-4 * abs(loss_ref)
     for name, a, b in zip(["W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4"], mlp_ref.unflatten(g),
                           mlp_ref.unflatten(g_ref)):
-        assert _rel(a, b) < 3e-2, (name, _rel(a, b))
+        assert _rel(a, b) < 3e-3, (name, _rel(a, b))
     m.status()
 
 
@@ -52,8 +54,14 @@ def test_training_reduces_loss(cuda):
     m = cm.Mlp(1024, seed=5)
     n = 1024
     recs, fam = _batch(8 * n, 7)
-    d = recs["dir"][:, :15].astype(np.float32)
-    y = (0.3 * (d[:, 0] - d[:, 3]) + 0.2 * np.maximum(d[:, 5] - 2, 0) + 0.1 * fam).astype(np.float32)
+    # a target the features determine: counts of x components equal to 4
+    # and of y components equal to 0, and the family
+    d = recs["dir"][:, :15]
+    p = np.array(mlp_ref.FAMILY_P)[fam]
+    ax = np.arange(15)[None, :]
+    n4x = ((d == 4) & (ax < p[:, None])).sum(1)
+    n0y = ((d == 0) & (ax >= p[:, None]) & (ax < 2 * p[:, None] - 1)).sum(1)
+    y = (0.3 * n4x - 0.2 * n0y + 0.1 * fam).astype(np.float32)
     d_in, d_fam, d_y = cmfw.to_device(recs), torch.from_numpy(fam).cuda(), torch.from_numpy(y).cuda()
     loss = torch.zeros(1, dtype=torch.float32, device="cuda")
     first = None

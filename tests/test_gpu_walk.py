@@ -67,10 +67,16 @@ def _limit_parity(desc, recs, g, src, o, N, h, rtol=1e-9):
     # exact ratios move by 4 ulps) is not far below rtol decides by rounding
     # which build lands within rtol
     noisy = ~(v["floor"] <= rtol / 100)
-    # a row fails only where the reference's own value is exact to rtol and
-    # the GPU's is not; elsewhere both are rounding noise of an
+    with np.errstate(invalid="ignore", over="ignore"):
+        g_err = np.abs(g["limit"][far] - L) / np.abs(L)
+        o_err = np.abs(o["limit"][far] - L) / np.abs(L)
+    # a row fails only where the reference's own value is exact to rtol, the
+    # GPU's is not, and the GPU's error is more than ten times the
+    # reference's (two walks whose errors both sit near rtol land on either
+    # side of it by chance); elsewhere both are rounding noise of an
     # ill-conditioned walk (or the estimator has no exact value)
-    bad = far[~(g_ok | undefined | noisy | ~o_ok)]
+    worse = ~(g_err <= 10.0 * o_err)
+    bad = far[~(g_ok | undefined | noisy | ~o_ok | ~worse)]
     assert len(bad) == 0, [(int(t), float(g["limit"][t]), float(o["limit"][t])) for t in bad[:5]]
     assert g_ok.sum() >= o_ok.sum() - 1 - len(far) // 100
     return len(far)
@@ -157,9 +163,36 @@ def test_f64_cfg2_batch_matches_oracle(cuda):
     m = g["valid"] == 1
     assert 30 <= m.sum() <= 100
     _limit_parity(desc, recs, g, src, o, 1000, 50)
-    for k in ("p", "q", "log_scale"):
-        _close_fraction(g[k][m], o[k][m], 1e-9, k)
+    _exact_pq_parity(desc, recs, g, o, m)
     _tail_parity(g, o, 1e-11, 1e-4)
+
+
+def _exact_pq_parity(desc, recs, g, o, m, n_max=300):
+    """p / q at depth N against the exact ratio on (up to n_max of) the
+    rows m: where many walks are ill-conditioned (the exact q many orders
+    below the matrix norm) the oracle's sequential f64 walk is no reference
+    for p and q, so both are compared with the exact value -- the GPU is
+    within 1e-12 and 1e-10 on at least as many rows as the oracle -- and
+    log_scale is compared where the two agree on p / q."""
+    from cmfw import exact
+    with np.errstate(invalid="ignore", divide="ignore"):
+        same = np.abs(g["p"] / g["q"] - o["p"] / o["q"]) <= 1e-9 * np.abs(o["p"] / o["q"])
+    both = m & same
+    if both.any():
+        _close_fraction(g["log_scale"][both], o["log_scale"][both], 1e-9, "log_scale")
+    idx = np.nonzero(m & (g["q"] != 0) & (o["q"] != 0))[0][:n_max]
+    ratios, _ = exact.exact_ratios(desc, recs[idx], 1000, 50, K0=1024)
+    eg, eo = [], []
+    for t, rs in zip(idx, ratios):
+        if rs is None or rs[2] == "inf" or rs[2] == 0:
+            continue
+        ex = float(rs[2])
+        eg.append(abs(g["p"][t] / g["q"][t] - ex) / abs(ex))
+        eo.append(abs(o["p"][t] / o["q"][t] - ex) / abs(ex))
+    eg, eo = np.array(eg), np.array(eo)
+    assert len(eg) >= 20
+    for bar in (1e-12, 1e-10):
+        assert (eg <= bar).sum() >= (eo <= bar).sum(), (bar, eg.tolist(), eo.tolist())
 
 
 def test_df64_tail_matches_oracle(cuda):

@@ -103,10 +103,13 @@ def test_exact_estimator_matches_reference_formula():
 
 def test_proposal_helpers():
     from cmfw import proposal as prop
-    t = prop.delta_target(np.array([0.0, 1.0, -1.0, 5397.0]))
-    assert t.dtype == np.float32
-    assert t[0] == 0.0 and abs(t[1] - np.log(2.0)) < 1e-6 and abs(t[2] + np.log(2.0)) < 1e-6
-    assert t[3] < 9.0 and prop.VALID_NAN < -1.0 and prop.FLOOR < prop.VALID_NAN
+    valid = np.array([1, 1, 1, 0, 1, 1, 1, 1], bool)
+    delta = np.array([0.5, 9.0, np.nan, 99.0, 3.0, -1.0, 7.0, np.inf])
+    t, w, thr = prop.top_target(valid, delta, top_q=0.2)
+    # finite deltas of valid walks: 0.5, 9, 3, -1, 7; the top 20% is 9
+    assert thr == np.quantile([0.5, 9.0, 3.0, -1.0, 7.0], 0.8)
+    assert t.tolist() == [0, 1, 0, 0, 0, 0, 0, 0] and t.dtype == np.float32
+    assert w[1] == 7.0 and (np.delete(w, 1) == 1.0).all()
     idx, d = prop.top_k(np.array([10, 11, 12, 13]), np.array([0.5, 3.0, -1.0, 3.0]), 2)
     assert idx.tolist() == [11, 13] and d.tolist() == [3.0, 3.0]
     assert prop.recall([1, 2, 3], [3, 4]) == 0.5
