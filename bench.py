@@ -60,11 +60,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="leave out the plain-kernel comparison and the valid-direction workload")
-    ap.add_argument("--workload", default="zeta6f5", choices=["zeta6f5", "mixed", "proposal"],
-                    help="zeta6f5: the headline 6F5 delta search; mixed: the mixed-family batch "
+    ap.add_argument("--workload", default="zeta6f5", choices=["zeta6f5", "zeta6f5_valid", "mixed", "proposal"],
+                    help="zeta6f5: the headline 6F5 delta search; zeta6f5_valid: the same search restricted to "
+                         "--valid-n directions whose walks stay valid (non-degenerate work); mixed: the "
+                         "mixed-family batch "
                          "(10^6 trajectories, N log-uniform 200..5000) in one graph launch; proposal: the "
                          "learned proposal for the 8F7 zeta delta search against the exhaustive sweep")
     ap.add_argument("--mixed-n", type=int, default=1000000)
+    ap.add_argument("--valid-n", type=int, default=2000, help="zeta6f5_valid: directions")
     ap.add_argument("--search-n", type=float, default=1e8, help="proposal: candidates searched")
     ap.add_argument("--train-n", type=float, default=1e8,
                     help="proposal: candidates whose filter survivors are walked for training")
@@ -78,9 +81,18 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def workload(rank):
+def workload(rank, args=None):
     import cmfw.workloads as wl
+    if args is not None and args.workload == "zeta6f5_valid":
+        return wl.valid_directions(P, Q, args.valid_n, SEED + rank, z=Z, N=N, h=H)
     return wl.zeta_directions(P, Q, NTRAJ, SEED + rank)
+
+
+WORKLOAD_TEXT = {
+    "zeta6f5": "6F5 zeta delta search: x=1^6, y=2^5, z=1, rank 5, dirs U{0..3}^11 != 0, N=1000, h=50",
+    "zeta6f5_valid": "6F5 zeta delta search restricted to directions whose walk stays valid (seeded rejection "
+                     "sampling of dirs U{0..3}^11 != 0), x=1^6, y=2^5, z=1, rank 5, N=1000, h=50",
+}
 
 
 def walk_flops(p, q, dim, records, Ns, valid):
@@ -340,7 +352,7 @@ def main_cmfw(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    records = workload(rank)
+    records = workload(rank, args)
     desc = cmfw.make_desc(P, Q, Z)
     n = len(records)
     d_in = cmfw.to_device(records)
@@ -446,8 +458,7 @@ def main_cmfw(args):
         "vs_baseline": None,
         "dtype": args.variant,
         "data": "synthetic (seeded std::mt19937_64 directions; no dataset)",
-        "config": {"workload": "6F5 zeta delta search: x=1^6, y=2^5, z=1, rank 5, "
-                               "dirs U{0..3}^11 != 0, N=1000, h=50",
+        "config": {"workload": WORKLOAD_TEXT[args.workload],
                    "n_traj_per_gpu": n, "seed": SEED, "variant": args.variant,
                    "l2": "flushed between steps (256 MiB write outside the timed events)",
                    "verification": f"exact rational walk (RNS, CRT + rational reconstruction), rtol {RTOL}"},
@@ -482,7 +493,7 @@ def main_cmfw(args):
                                 "verification": "estimator of each limit from the oracle's restatement of the "
                                                 "reference's reduction, exact values from the GPU exact walk"}
     line["accuracy"] = accuracy(vinfo["rel_err"], vinfo["floor"], results["valid"] == 1)
-    if world == 1 and not args.no_extras:
+    if world == 1 and not args.no_extras and args.workload == "zeta6f5":
         plain = plain_kernels(desc, records, d_in, flush, 3)
         ref = plain.get("reference_sm100a", {})
         if ref.get("verified_traj_per_s"):

@@ -36,12 +36,12 @@ def test_trained_proposal_beats_the_same_budget_without_it(cuda):
     for i, d in zip(p_idx.tolist(), p_d.tolist()):
         if i in sweep_delta:
             assert d == sweep_delta[i]
-    # the best trajectories' limits against the exact rational walk: each
-    # verifies at 1e-10 unless its estimator is ill-conditioned (the largest
-    # deltas come from walks whose ratios have converged so far that
-    # Aitken's second difference is rounding noise: its rounding floor is
-    # then above the tolerance, and no double-precision walk does better)
+    # the best trajectories' limits against the exact rational walk. The
+    # largest deltas of a floating-point sweep include walks whose result
+    # has lost the subdominant solution (the float ratios stop moving, so
+    # delta is huge, while the exact limit is elsewhere, by 1e-5 relative
+    # here): telling those apart is the exact confirmation's job, so it must
+    # give a finite verdict for each and confirm some
     v = S.confirm(truth[:5], detail=True)
-    ok = v["verified"] | (v["floor"] > 1e-10)
-    assert ok.all(), (v["rel_err"], v["floor"])
-    assert v["verified"].sum() >= 1
+    assert np.isfinite(v["rel_err"]).all(), v["rel_err"]
+    assert v["verified"].sum() >= 2, (v["rel_err"], v["floor"])
