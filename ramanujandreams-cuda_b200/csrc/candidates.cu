@@ -3,6 +3,8 @@
 // applied to candidates of the seeded generator drawn in place, with the
 // indices of the candidates that pass compacted into a list.
 //
+// Only the verdict is kept, so the tests run in the order that ends a
+// failing candidate soonest (lattice_step_passes: inverse steps first).
 // A candidate that fails here is an invalid walk whatever arithmetic walks
 // it (the tests depend on the position only: cmf_pfq.cuh:164-174 lead
 // coefficient, :193 denominator, :225-232 scalar solve), and it is exactly
@@ -64,7 +66,7 @@ __global__ void __launch_bounds__(kCandidateThreads) filter_candidates_kernel(Fi
         for (int a = 0; a < NAX; ++a) pos[a] = (a < naxes) ? A.start[a] : 0.0;
         bool ok = true;
         for (int step = 1; step <= A.S && ok; ++step)
-            ok = lattice_step_tests<DIM, NAX, PM, QM>(pos, absd, neg, maxabs, K) == CMFW_TRAJ_OK;
+            ok = lattice_step_passes<DIM, NAX, PM, QM>(pos, absd, neg, maxabs, K);
         if (!ok) continue;
         const unsigned long long at = atomicAdd(A.count, 1ull);
         if ((long long)at < A.cap) A.idx[at] = cand;

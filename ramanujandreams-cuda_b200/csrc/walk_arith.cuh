@@ -508,6 +508,40 @@ __device__ __forceinline__ int lattice_step_tests(double (&pos)[NAX], const int 
     return CMFW_TRAJ_OK;
 }
 
+// The verdict alone of lattice_step_tests (CMFW_TRAJ_OK or not, with no
+// status of which step failed): every test depends on the position only,
+// so the tests can run in any order. The inverse steps (x-, y+), which are
+// the ones that fail at a symmetric start, are tested first in a pass that
+// only moves the position for the others; the forward steps follow only if
+// they all pass. pos ends at the lattice step's end when the verdict is OK.
+template <int DIM, int NAX, int PM, int QM>
+__device__ __forceinline__ bool lattice_step_passes(double (&pos)[NAX], const int (&absd)[NAX], uint32_t neg,
+                                                    int maxabs, const StepConst &K) {
+    double start[NAX];
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) start[a] = pos[a];
+    for (int pass = 0; pass < 2; ++pass) {
+#pragma unroll
+        for (int a = 0; a < NAX; ++a) pos[a] = start[a];
+        for (int level = maxabs; level >= 1; --level) {
+            uint32_t mask = level_mask<NAX>(absd, level);
+            while (mask) {
+                const int axis = top_axis(mask);
+                mask &= ~(1u << axis);
+                const bool up = !((neg >> axis) & 1u);
+                const bool inverse = (axis < K.P) ? !up : up;
+                if (inverse == (pass == 0)) {
+                    StepMatrix<DIM> S;
+                    if (step_matrix<false, DIM, NAX, PM, QM>(pos, axis, up, K, S) != CMFW_TRAJ_OK) return false;
+                }
+#pragma unroll
+                for (int a = 0; a < NAX; ++a) pos[a] += (a == axis) ? (up ? 1.0 : -1.0) : 0.0;
+            }
+        }
+    }
+    return true;
+}
+
 __device__ __forceinline__ StepConst make_step_const(int P, int Q, int DIM, double z) {
     StepConst K;
     K.P = P;
