@@ -61,11 +61,12 @@ def parse():
     ap.add_argument("--no-extras", action="store_true",
                     help="leave out the plain-kernel comparison and the valid-direction workload")
     ap.add_argument("--workload", default="zeta6f5",
-                    choices=["zeta6f5", "zeta6f5_valid", "limit3f2", "mixed", "proposal"],
+                    choices=["zeta6f5", "zeta6f5_valid", "limit3f2", "rns8f7", "mixed", "proposal"],
                     help="zeta6f5: the headline 6F5 delta search; zeta6f5_valid: the same search restricted to "
                          "--valid-n directions whose walks stay valid (non-degenerate work); limit3f2: "
                          "3F2 z=1/2 limit walks from 10,000 starts U{1..10}, direction 1^5 (the CPU-baseline "
-                         "configuration); mixed: the "
+                         "configuration); rns8f7: the 8F7 zeta RNS walk (dirs 1^15 + U{0..2}^15) at N 1000 "
+                         "and 4000 with 8 and 16 moduli, beside the reference's own RNS kernel; mixed: the "
                          "mixed-family batch "
                          "(10^6 trajectories, N log-uniform 200..5000) in one graph launch; proposal: the "
                          "learned proposal for the 8F7 zeta delta search against the exhaustive sweep")
@@ -587,6 +588,80 @@ def main_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def main_rns(args):
+    """8F7 at the zeta point (x = 1^8, y = 2^7, z = 1, rank 7), 10,000
+    directions 1^15 + U{0..2}^15 (seeded), limit mode, the compat RNS walk
+    (the reference's cmf_walk_rns semantics: 30-bit moduli, rounded column,
+    2-modulus CRT every 100 steps) at N = 1000 and 4000 with 8 and 16
+    moduli. Per configuration: traj/s of this project's kernel and of the
+    reference's own walk_kernel_rns built for sm_100a on the same buffers
+    (CUDA events, L2 flushed), the valid count, bit-exactness of limit, p
+    and q against the oracle on every valid row, and at N = 1000 the exact
+    ratios of up to 8 valid walks (exact walk + device reconstruction)."""
+    import torch
+    import cmfw
+    import cmfw.workloads as wl
+    import oracle
+    from cmfw import exact
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    p, q, z, n = 8, 7, 1.0, NTRAJ
+    recs = wl.zeta_directions(p, q, n, SEED, lo=0, hi=2, offset=1)
+    desc = cmfw.make_desc(p, q, z)
+    d_in = cmfw.to_device(recs)
+    d_out = cmfw.out_buffer(n)
+    d_ref = torch.empty((n, 56), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    res = {}
+    for Nd in (1000, 4000):
+        for K in (8, 16):
+            mine = lambda: cmfw.launch_walk("rns", desc, d_in, d_out, n, Nd, H, n_primes=K)
+            for _ in range(max(args.warmup, 1)):
+                mine()
+            torch.cuda.synchronize()
+            t = time_events(mine, args.steps, flush)
+            g = cmfw.records_from_device(d_out, n)
+            m = np.nonzero(g["valid"] == 1)[0]
+            o = oracle.walk("rns", p, q, z, Nd, H, recs[m], n_primes=K, fused=True)
+            bitexact = all(np.array_equal(g[k][m], o[k], equal_nan=True) for k in ("limit", "p", "q")) and \
+                (o["valid"] == 1).all()
+            entry = {"ms_per_step": t * 1e3, "traj_per_s": n / t, "n_valid": int(len(m)),
+                     "bit_exact_vs_oracle": bool(bitexact)}
+            if oracle.have_ref_gpu("rns"):
+                ref = lambda: oracle.ref_gpu_launch("rns", p, q, z, Nd, H, d_in.data_ptr(), d_ref.data_ptr(), n,
+                                                    stream=stream, n_primes=K)
+                ref()
+                torch.cuda.synchronize()
+                tr = time_events(ref, args.steps, flush)
+                rout = d_ref.cpu().numpy().reshape(-1).view(cmfw.OUT_DTYPE)
+                entry["reference_sm100a"] = {"ms_per_step": tr * 1e3, "traj_per_s": n / tr,
+                                             "same_valid": bool(np.array_equal(rout["valid"], g["valid"])),
+                                             "same_results": bool(all(np.array_equal(rout[k][m], g[k][m], equal_nan=True)
+                                                                      for k in ("limit", "p", "q")))}
+            if len(m) and Nd == 1000:
+                # exact ratios of (up to 8 of) the valid walks: exact walk + device reconstruction
+                sub = m[:8]
+                ratios, K_used = exact.exact_ratios(desc, recs[sub], Nd, H)
+                entry["exact_ratios"] = {"rows": int(len(sub)), "determined": int(sum(r is not None for r in ratios)),
+                                         "primes_max": int(K_used.max())}
+            res[f"N{Nd}_K{K}"] = entry
+    head = res["N1000_K8"]
+    line = {
+        "metric": "8F7 zeta RNS walk traj/s on 1 B200 (compat semantics, bit-exact vs the reference)",
+        "value": head["traj_per_s"], "unit": "traj/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": head["ms_per_step"], "higher_is_better": True, "dtype": "u32 residues",
+        "data": "synthetic (seeded std::mt19937_64 directions)",
+        "config": {"workload": "8F7 zeta limit: x=1^8, y=2^7, z=1, rank 7, dirs 1^15 + U{0..2}^15, h=50, "
+                               "N in {1000, 4000}, moduli in {8, 16}", "n_traj": n, "seed": SEED,
+                   "l2": "flushed between steps"},
+        "configs": res,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main_mixed(args):
     """Mixed-family batch: 3F2/4F3/5F4/6F5/8F7 x z in {1/2, 1}, starts
     U{1..10}, directions U{0..3} (not all zero), N log-uniform in 200..5000,
@@ -719,6 +794,8 @@ if __name__ == "__main__":
         main_reference(a)
     elif a.workload == "mixed":
         main_mixed(a)
+    elif a.workload == "rns8f7":
+        main_rns(a)
     elif a.workload == "proposal":
         main_proposal(a)
     else:

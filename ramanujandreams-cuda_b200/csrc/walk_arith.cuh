@@ -508,21 +508,56 @@ __device__ __forceinline__ int lattice_step_tests(double (&pos)[NAX], const int 
     return CMFW_TRAJ_OK;
 }
 
-// The verdict alone of lattice_step_tests (CMFW_TRAJ_OK or not, with no
-// status of which step failed): every test depends on the position only,
-// so the tests can run in any order. The inverse steps (x-, y+), which are
-// the ones that fail at a symmetric start, are tested first in a pass that
-// only moves the position for the others; the forward steps follow only if
-// they all pass. pos ends at the lattice step's end when the verdict is OK.
+// The position before axis step (level, axis) of a lattice step that
+// starts at pos, in closed form: levels run from max|dir| down and, within
+// a level, axes from the highest down (cmf_pfq.cuh:313-320), so axis a has
+// moved max(0, |d_a| - level) times at earlier levels and once more at this
+// level if it comes before `axis` (a > axis, |d_a| >= level). The values
+// are integers, the same as stepping one axis at a time.
+template <int NAX>
+__device__ __forceinline__ void position_at(const double (&pos)[NAX], const int (&absd)[NAX], uint32_t neg,
+                                            int level, int axis, double (&out)[NAX]) {
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) {
+        const int moved = max(0, absd[a] - level) + ((a > axis && absd[a] >= level) ? 1 : 0);
+        out[a] = pos[a] + (double)(((neg >> a) & 1u) ? -moved : moved);
+    }
+}
+
+// lattice_step_tests with each step's position formed in closed form
+// (position_at) instead of moved step by step: the same statuses, the
+// earliest failing step's, and pos advanced by the whole step when it
+// passes.
+template <int DIM, int NAX, int PM, int QM>
+__device__ __forceinline__ int lattice_step_status(double (&pos)[NAX], const int (&absd)[NAX], uint32_t neg,
+                                                   int maxabs, const StepConst &K) {
+    for (int level = maxabs; level >= 1; --level) {
+        uint32_t mask = level_mask<NAX>(absd, level);
+        while (mask) {
+            const int axis = top_axis(mask);
+            mask &= ~(1u << axis);
+            const bool up = !((neg >> axis) & 1u);
+            double at[NAX];
+            position_at<NAX>(pos, absd, neg, level, axis, at);
+            StepMatrix<DIM> S;
+            const int st = step_matrix<false, DIM, NAX, PM, QM>(at, axis, up, K, S);
+            if (st != CMFW_TRAJ_OK) return st;
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) pos[a] += (double)(((neg >> a) & 1u) ? -absd[a] : absd[a]);
+    return CMFW_TRAJ_OK;
+}
+
+// The verdict alone (pass or not, no status): every test depends on the
+// position only, so the tests can run in any order. The inverse steps
+// (x-, y+), which are the ones that fail at a symmetric start, are tested
+// first, then the forward steps; positions in closed form. pos advances by
+// the whole step when it passes.
 template <int DIM, int NAX, int PM, int QM>
 __device__ __forceinline__ bool lattice_step_passes(double (&pos)[NAX], const int (&absd)[NAX], uint32_t neg,
                                                     int maxabs, const StepConst &K) {
-    double start[NAX];
-#pragma unroll
-    for (int a = 0; a < NAX; ++a) start[a] = pos[a];
     for (int pass = 0; pass < 2; ++pass) {
-#pragma unroll
-        for (int a = 0; a < NAX; ++a) pos[a] = start[a];
         for (int level = maxabs; level >= 1; --level) {
             uint32_t mask = level_mask<NAX>(absd, level);
             while (mask) {
@@ -530,15 +565,16 @@ __device__ __forceinline__ bool lattice_step_passes(double (&pos)[NAX], const in
                 mask &= ~(1u << axis);
                 const bool up = !((neg >> axis) & 1u);
                 const bool inverse = (axis < K.P) ? !up : up;
-                if (inverse == (pass == 0)) {
-                    StepMatrix<DIM> S;
-                    if (step_matrix<false, DIM, NAX, PM, QM>(pos, axis, up, K, S) != CMFW_TRAJ_OK) return false;
-                }
-#pragma unroll
-                for (int a = 0; a < NAX; ++a) pos[a] += (a == axis) ? (up ? 1.0 : -1.0) : 0.0;
+                if (inverse != (pass == 0)) continue;
+                double at[NAX];
+                position_at<NAX>(pos, absd, neg, level, axis, at);
+                StepMatrix<DIM> S;
+                if (step_matrix<false, DIM, NAX, PM, QM>(at, axis, up, K, S) != CMFW_TRAJ_OK) return false;
             }
         }
     }
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) pos[a] += (double)(((neg >> a) & 1u) ? -absd[a] : absd[a]);
     return true;
 }
 

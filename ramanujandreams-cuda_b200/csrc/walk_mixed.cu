@@ -466,11 +466,16 @@ cmfw_mixed_tuning default_tuning(int n_descs) {
 }
 
 // Candidate c of the autotuner's whole-batch stage: -2 the plain 256-thread
-// grid everywhere (the fixed baseline), -1 the per-family choices, 0..8
-// tile c (block blocks[c / 3], grab grabs[c % 3]) for every family.
+// grid everywhere (the fixed baseline), -1 the per-family choices, -3 the
+// default tiles, -4 / -5 the default tiles / the per-family choices with the
+// singularity prescan, 0..8 tile c (block blocks[c / 3], grab grabs[c % 3])
+// for every family.
+constexpr int kFirstCandidate = -5;
 cmfw_mixed_tuning joint_candidate(const cmfw_mixed_tuning &per_family, int c, int n_descs, const int *blocks,
                                   const int *grabs) {
     cmfw_mixed_tuning t = per_family;
+    if (c == -3 || c == -4) t = default_tuning(n_descs);
+    if (c == -4 || c == -5) t.prescan = 1;
     if (c == -2) t.persistent = 0;
     if (c >= 0)
         for (int f = 0; f < n_descs; ++f) {
@@ -607,7 +612,7 @@ cmfw_status cmfw_mixed_autotune(const cmfw_desc *descs, int n_descs, const cmfw_
         Mj.next = d_snext;
         const cmfw_mixed_tuning per_family = *out;
         std::vector<std::pair<float, int>> timed;  // (sample ms, candidate)
-        for (int c = -2; c < 9 && e == cudaSuccess; ++c) {
+        for (int c = kFirstCandidate; c < 9 && e == cudaSuccess; ++c) {
             const cmfw_mixed_tuning t = joint_candidate(per_family, c, n_descs, blocks, grabs);
             float ms = 0.f;
             for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {  // warm-up, then timed
@@ -621,25 +626,31 @@ cmfw_status cmfw_mixed_autotune(const cmfw_desc *descs, int n_descs, const cmfw_
             if (e == cudaSuccess) timed.push_back({ms, c});
         }
         // A sample ranks the candidates but can misjudge the whole batch's
-        // tails: the fastest three on the sample and the fixed baseline (the
-        // plain 256-thread grid, c = -2) are timed on the whole batch, and
-        // the fastest of those is kept -- so the tuning never loses to the
-        // baseline by more than the timing noise.
+        // tails: the fastest three on the sample, the default tiles (c = -3)
+        // and the fixed baseline (the plain 256-thread grid, c = -2) are
+        // timed on the whole batch, and the fastest of those is kept -- so
+        // the tuning never loses to the default or the baseline by more than
+        // the timing noise.
         std::sort(timed.begin(), timed.end());
         std::vector<int> finalists;
         for (size_t i = 0; i < timed.size() && finalists.size() < 3; ++i) finalists.push_back(timed[i].second);
-        if (std::find(finalists.begin(), finalists.end(), -2) == finalists.end()) finalists.push_back(-2);
+        for (int must : {-2, -3})
+            if (std::find(finalists.begin(), finalists.end(), must) == finalists.end()) finalists.push_back(must);
         float best = 1e30f;
         for (int c : finalists) {
             if (e != cudaSuccess) break;
             const cmfw_mixed_tuning t = joint_candidate(per_family, c, n_descs, blocks, grabs);
-            float ms = 0.f;
-            for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+            // warm-up, then the better of two timed runs (the finalists are
+            // often within a few per cent of each other)
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+                float m1 = 0.f;
                 e = cudaEventRecord(a, s);
                 if (e == cudaSuccess) e = enqueue_mixed(M, L, variant, t, s);
                 if (e == cudaSuccess) e = cudaEventRecord(b, s);
                 if (e == cudaSuccess) e = cudaEventSynchronize(b);
-                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&m1, a, b);
+                if (rep > 0 && m1 < ms) ms = m1;
             }
             if (e == cudaSuccess && ms < best) {
                 best = ms;

@@ -400,15 +400,29 @@ def test_df64_accurate_against_exact(cuda):
     assert np.median(e["gff"]) <= 1e-9
 
 
-def test_df64_compat_matches_oracle(cuda):
-    p, q, z = 4, 3, 1.0
-    recs = oracle.make_inputs(p, q, 100, 0, True)
+@pytest.mark.parametrize("p,q", FAMILIES)
+@pytest.mark.parametrize("z,mode,zeta", [(1.0, 0, True), (0.5, 0, False), (0.5, 1, False)])
+def test_df64_compat_matches_oracle(cuda, p, q, z, mode, zeta):
+    """The reference's own df64 arithmetic (float reciprocals,
+    cmf_walk_df64.cu:35-349) on the GPU against the oracle's restatement of
+    it: validity identical; limit and q within 1e-7 on the valid rows where
+    the walk is conditioned well enough for a ~1e-9 arithmetic (the
+    oracle's own f64 walk agrees with its df64 walk to 1e-6) -- elsewhere
+    both are rounding noise of a 48-bit walk."""
+    recs = oracle.make_inputs(p, q, 300, mode, zeta)[:100]
     desc = cmfw.make_desc(p, q, z)
     g = cmfw.walk("df64", desc, recs, 1000, 50, flags=cmfw.F_DF64_COMPAT)
     o = oracle.walk("df64", p, q, z, 1000, 50, recs, fused=True)
+    o64 = oracle.walk("f64", p, q, z, 1000, 50, recs, fused=True)
     np.testing.assert_array_equal(g["valid"], o["valid"])
-    np.testing.assert_allclose(g["limit"], o["limit"], rtol=1e-7)
-    np.testing.assert_allclose(g["q"], o["q"], rtol=1e-7)
+    m = (o["valid"] == 1) & np.isfinite(o["limit"]) & np.isfinite(o64["limit"])
+    with np.errstate(invalid="ignore"):
+        m &= np.abs(o["limit"] - o64["limit"]) <= 1e-6 * np.abs(o64["limit"])
+        m &= np.abs(o["q"] - o64["q"]) <= 1e-6 * np.abs(o64["q"])
+    if not m.any():
+        return
+    np.testing.assert_allclose(g["limit"][m], o["limit"][m], rtol=1e-7)
+    np.testing.assert_allclose(g["q"][m], o["q"][m], rtol=1e-7)
 
 
 @pytest.mark.parametrize("variant,rtol", [("f64", 1e-11), ("df64", 1e-9)])
