@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(kCandidateThreads) filter_candidates_kernel(Fi
     const int Q = (P_ > 0) ? Q_ : A.q;
     const int naxes = P + Q;
     const StepConst K = make_step_const(P, Q, DIM, A.z);
+    const SmallMod mod((uint32_t)A.span);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < A.n; c += stride) {
         const long long cand = A.first + c;
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(kCandidateThreads) filter_candidates_kernel(Fi
         for (int a = 0; a < NAX; ++a) {
             if ((a & 3) == 0) d = candidate_draw(A.seed, cand, a >> 2);
             int v = 0;
-            if (a < naxes) v = A.lo + (int)(((d >> (16 * (a & 3))) & 0xFFFFull) % (uint64_t)A.span);
+            if (a < naxes) v = A.lo + (int)mod((uint32_t)((d >> (16 * (a & 3))) & 0xFFFFull));
             if (v < 0) neg |= 1u << a;
             absd[a] = v < 0 ? -v : v;
             maxabs = max(maxabs, absd[a]);

@@ -22,9 +22,25 @@ __host__ __device__ inline uint64_t candidate_draw(uint64_t seed, long long idx,
     return splitmix64(seed ^ ((uint64_t)idx * 4ull + (uint64_t)w) * 0xD1B54A32D192ED03ull);
 }
 
-__host__ __device__ inline int candidate_component(uint64_t seed, long long idx, int a, int lo, int span) {
+// x mod d for x < 2^16 and d >= 1 without a division. With
+// m = floor((2^32 - 1) / d) + 1 (ceil(2^32 / d), or 2^32 / d for d a power
+// of two), x m / 2^32 = x / d + x e / 2^32 with 0 <= e < 1. For d <= 2^16,
+// x e / 2^32 < 2^-16 <= 1 / d, less than the distance from x / d to the
+// next integer, so floor(x m / 2^32) = floor(x / d). For d > 2^16, m <= 2^16
+// and x m < 2^32: the quotient is 0 = floor(x / d).
+struct SmallMod {
+    uint32_t d;
+    uint64_t m;
+    __host__ __device__ explicit SmallMod(uint32_t d_) : d(d_), m((uint64_t)(0xFFFFFFFFu / d_) + 1ull) {}
+    __host__ __device__ uint32_t operator()(uint32_t x) const { return x - (uint32_t)(((uint64_t)x * m) >> 32) * d; }
+};
+
+__host__ __device__ inline int candidate_component(uint64_t seed, long long idx, int a, int lo, const SmallMod &mod) {
     const uint64_t w = candidate_draw(seed, idx, a >> 2);
-    return lo + (int)(((w >> (16 * (a & 3))) & 0xFFFFull) % (uint64_t)span);
+    return lo + (int)mod((uint32_t)((w >> (16 * (a & 3))) & 0xFFFFull));
+}
+__host__ __device__ inline int candidate_component(uint64_t seed, long long idx, int a, int lo, int span) {
+    return candidate_component(seed, idx, a, lo, SmallMod((uint32_t)span));
 }
 
 // Network features of a direction d[0..naxes) of family `family` (0..4 =

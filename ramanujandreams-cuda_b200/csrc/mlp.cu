@@ -465,7 +465,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256) mlp_score_fused
     bool ok = true;
     const long long ntiles = (a.n + 127) / 128;
     const int nclusters = gridDim.x / 2;
-    const int span = a.hi - a.lo + 1;
+    const SmallMod mod((uint32_t)(a.hi - a.lo + 1));
     const int trow = (warp & 3) * 32 + lane;  // accumulator lane = tile row
     const int tcol = (warp >> 2) * 64;        // this thread's 64 accumulator columns
 
@@ -486,8 +486,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256) mlp_score_fused
                 for (int w = 0; w < 4; ++w) {
                     const uint64_t d = candidate_draw(a.seed, idx, w);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        comp[4 * w + q] = a.lo + (int)((uint32_t)((d >> (16 * q)) & 0xFFFFull) % (uint32_t)span);
+                    for (int q = 0; q < 4; ++q) comp[4 * w + q] = a.lo + (int)mod((uint32_t)((d >> (16 * q)) & 0xFFFFull));
                 }
                 direction_features([&](int k) { return comp[k]; }, a.naxes, a.family, v);
             }
