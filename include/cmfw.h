@@ -368,8 +368,9 @@ cmfw_status cmfw_filter_candidates(const cmfw_desc *desc, uint64_t seed, long lo
 /* Records of the candidates d_idx[0..n) of the same generator, start d_start. */
 cmfw_status cmfw_candidate_records(uint64_t seed, const long long *d_idx, int n, int naxes, int lo, int hi,
                                    const double *d_start, cmfw_traj_in *d_out, void *stream);
-/* Indices of the k largest of d_scores[0..n) (ties at the threshold
- * included, at most cap written) into d_idx, their number in *h_count;
+/* Indices of the k largest of d_scores[0..n) (n < 2^32; equal scores
+ * ordered by lower index, so exactly min(k, n) are selected; at most cap
+ * written, in no particular order) into d_idx, their number in *h_count;
  * synchronises. */
 cmfw_status cmfw_select_top(const float *d_scores, long long n, long long k, long long *d_idx, int cap,
                             int *h_count, void *stream);

@@ -134,7 +134,8 @@ def candidate_records(seed, d_idx, naxes, lo, hi, start, stream=None):
 
 
 def select_top(d_scores, k, cap=None):
-    """Indices (int64 tensor) of the k largest scores, ties at the threshold included."""
+    """Indices (int64 tensor, unordered) of the k largest scores; equal
+    scores are taken in index order, so exactly min(k, n) are returned."""
     torch = api._torch()
     n = int(d_scores.numel())
     cap = int(cap or (2 * k + 1024))

@@ -35,12 +35,17 @@ struct SmallMod {
     __host__ __device__ uint32_t operator()(uint32_t x) const { return x - (uint32_t)(((uint64_t)x * m) >> 32) * d; }
 };
 
-__host__ __device__ inline int candidate_component(uint64_t seed, long long idx, int a, int lo, const SmallMod &mod) {
-    const uint64_t w = candidate_draw(seed, idx, a >> 2);
-    return lo + (int)mod((uint32_t)((w >> (16 * (a & 3))) & 0xFFFFull));
-}
-__host__ __device__ inline int candidate_component(uint64_t seed, long long idx, int a, int lo, int span) {
-    return candidate_component(seed, idx, a, lo, SmallMod((uint32_t)span));
+// Components 0..15 of candidate idx (16-bit field a & 3 of draw a >> 2,
+// reduced modulo the span, plus lo); a direction of naxes axes uses the
+// first naxes.
+__host__ __device__ inline void candidate_direction(uint64_t seed, long long idx, int lo, const SmallMod &mod,
+                                                    int comp[16]) {
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        const uint64_t d = candidate_draw(seed, idx, w);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) comp[4 * w + q] = lo + (int)mod((uint32_t)((d >> (16 * q)) & 0xFFFFull));
+    }
 }
 
 // Network features of a direction d[0..naxes) of family `family` (0..4 =

@@ -221,9 +221,10 @@ __global__ void candidate_features_kernel(uint64_t seed, long long first, int n,
     const int t = i / kIn, c = i % kIn;
     float v = 0.0f;
     if (t < n && c < 20) {
+        int comp[16];
+        candidate_direction(seed, first + t, lo, SmallMod((uint32_t)(hi - lo + 1)), comp);
         float f[20];
-        direction_features([&](int a) { return candidate_component(seed, first + t, a, lo, hi - lo + 1); }, naxes,
-                           family, f);
+        direction_features([&](int a) { return comp[a]; }, naxes, family, f);
         v = f[c];
     }
     X[i] = __float2bfloat16_rn(v);
@@ -233,9 +234,11 @@ __global__ void candidate_records_kernel(uint64_t seed, const long long *idx, in
                                          const double *start, cmfw_traj_in *out) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
+    int comp[16];
+    candidate_direction(seed, idx[t], lo, SmallMod((uint32_t)(hi - lo + 1)), comp);
     cmfw_traj_in r;
     for (int a = 0; a < CMFW_MAX_AXES; ++a) {
-        r.dir[a] = a < naxes ? candidate_component(seed, idx[t], a, lo, hi - lo + 1) : 0;
+        r.dir[a] = a < naxes ? comp[a] : 0;
         r.start[a] = a < naxes ? start[a] : 0.0;
     }
     out[t] = r;
@@ -345,24 +348,32 @@ __device__ __forceinline__ uint32_t score_key(float f) {
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-__global__ void score_hist_kernel(const float *score, long long n, uint32_t shift, uint32_t prefix,
-                                  uint32_t prefix_mask, unsigned long long *hist) {
+// Selection key of score i (n < 2^32): the score's key above the index's
+// complement, so keys are distinct and order by score, then by lower index.
+__device__ __forceinline__ uint64_t select_key(const float *score, long long i) {
+    return ((uint64_t)score_key(score[i]) << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)i);
+}
+
+// Histogram of the selection keys that match prefix under prefix_mask, by
+// their `bits` bits above `shift` (bits <= 11).
+__global__ void score_hist_kernel(const float *score, long long n, uint32_t shift, uint32_t bits, uint64_t prefix,
+                                  uint64_t prefix_mask, unsigned long long *hist) {
     __shared__ unsigned int h[2048];
     for (int i = threadIdx.x; i < 2048; i += blockDim.x) h[i] = 0;
     __syncthreads();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const uint32_t k = score_key(score[i]);
-        if ((k & prefix_mask) == prefix) atomicAdd(&h[(k >> shift) & 2047u], 1u);
+        const uint64_t k = select_key(score, i);
+        if ((k & prefix_mask) == prefix) atomicAdd(&h[(uint32_t)(k >> shift) & ((1u << bits) - 1u)], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < 2048; i += blockDim.x)
         if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
 }
 
-__global__ void select_kernel(const float *score, long long n, uint32_t kmin, long long *out, int cap,
+__global__ void select_kernel(const float *score, long long n, uint64_t kmin, long long *out, int cap,
                               int *count) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        if (score_key(score[i]) >= kmin) {
+        if (select_key(score, i) >= kmin) {
             const int pos = atomicAdd(count, 1);
             if (pos < cap) out[pos] = i;
         }
@@ -482,12 +493,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256) mlp_score_fused
             if (cand < a.n) {
                 const long long idx = a.idx ? __ldg(a.idx + cand) : a.first + cand;
                 int comp[16];
-#pragma unroll
-                for (int w = 0; w < 4; ++w) {
-                    const uint64_t d = candidate_draw(a.seed, idx, w);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) comp[4 * w + q] = a.lo + (int)mod((uint32_t)((d >> (16 * q)) & 0xFFFFull));
-                }
+                candidate_direction(a.seed, idx, a.lo, mod, comp);
                 direction_features([&](int k) { return comp[k]; }, a.naxes, a.family, v);
             }
 #pragma unroll
@@ -973,22 +979,25 @@ cmfw_status cmfw_candidate_records(uint64_t seed, const long long *d_idx, int n,
 
 cmfw_status cmfw_select_top(const float *d_scores, long long n, long long k, long long *d_idx, int cap, int *h_count,
                             void *stream) {
-    if (!d_scores || !d_idx || !h_count || k < 1 || cap < 1) return record_error(CMFW_EINVAL, "bad selection arguments");
+    if (!d_scores || !d_idx || !h_count || k < 1 || cap < 1 || n < 0 || n > 0xFFFFFFFFll)
+        return record_error(CMFW_EINVAL, "bad selection arguments");
     cudaStream_t s = (cudaStream_t)stream;
     unsigned long long *d_hist = nullptr;
     int *d_count = nullptr;
     cudaError_t e = cudaMalloc(&d_hist, 2048 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&d_count, sizeof(int));
-    // radix select of the k-th largest key: 11 + 11 + 10 bits
-    uint32_t prefix = 0, mask = 0;
+    // radix select of the k-th largest selection key, 11 + 11 + 10 bits of
+    // the score key then of the index part; it stops early once the
+    // threshold's bin holds exactly the keys still needed (k >= n: all)
+    uint64_t prefix = 0, mask = 0;
     long long need = k;
-    const uint32_t shifts[3] = {21, 10, 0};
-    const uint32_t widths[3] = {11, 11, 10};
+    const uint32_t shifts[6] = {53, 42, 32, 21, 10, 0};
+    const uint32_t widths[6] = {11, 11, 10, 11, 11, 10};
     std::vector<unsigned long long> h(2048);
-    for (int pass = 0; pass < 3 && e == cudaSuccess; ++pass) {
+    for (int pass = 0; pass < 6 && e == cudaSuccess && k < n; ++pass) {
         e = cudaMemsetAsync(d_hist, 0, 2048 * sizeof(unsigned long long), s);
         if (e != cudaSuccess) break;
-        score_hist_kernel<<<592, 256, 0, s>>>(d_scores, n, shifts[pass], prefix, mask, d_hist);
+        score_hist_kernel<<<592, 256, 0, s>>>(d_scores, n, shifts[pass], widths[pass], prefix, mask, d_hist);
         e = cudaMemcpyAsync(h.data(), d_hist, 2048 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) break;
@@ -998,8 +1007,9 @@ cmfw_status cmfw_select_top(const float *d_scores, long long n, long long k, lon
             if ((long long)h[b] >= need) break;
             need -= (long long)h[b];
         }
-        prefix |= (uint32_t)b << shifts[pass];
-        mask |= (uint32_t)(nb - 1) << shifts[pass];
+        prefix |= (uint64_t)b << shifts[pass];
+        mask |= (uint64_t)(nb - 1) << shifts[pass];
+        if ((long long)h[b] == need) break;  // every key of this bin is selected
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, sizeof(int), s);
     if (e == cudaSuccess) {

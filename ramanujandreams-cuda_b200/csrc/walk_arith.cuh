@@ -358,6 +358,57 @@ struct StepMatrix {
     bool inverse;
 };
 
+// The lead coefficient's singularity test (the one in step_matrix) without
+// the rest of the column, where the lead needs only the top two
+// coefficients of each theta product: dim >= p - 1 and dim >= q, which
+// holds for dim = p = q + 1 and for dim = p - 1 = q. theta_product forms
+// the top coefficient of prod_{j<n} (theta + v_j) as exactly 1 and the
+// next as the running sum ((v_0 + v_1) + v_2) + ... (each step a fused
+// multiply-add by the top coefficient 1), so both are reproduced exactly
+// here; column_poly then forms -z * px[dim] + py[dim - 1], which the
+// compiler may evaluate with one rounding (fused) or two. Both roundings
+// are tried: returns 1 (singular) or 0 (not) when they agree, -1 when
+// they disagree, the positions are not finite or the shape does not
+// qualify (the caller then forms the full column).
+template <int PM, int QM, int DIM>
+__device__ __forceinline__ int lead_verdict(const double (&xv)[PM], const double (&yv)[QM > 0 ? QM : 1], int P,
+                                            int Q, const StepConst &K) {
+    if (DIM < P - 1 || DIM < Q) return -1;
+    double sx = 0.0, sy = 0.0;
+#pragma unroll
+    for (int j = 0; j < PM; ++j)
+        if (j < P) sx = (j == 0) ? xv[0] : sx + xv[j];
+#pragma unroll
+    for (int i = 0; i < (QM > 0 ? QM : 1); ++i)
+        if (i < Q) sy = (i == 0) ? yv[0] : sy + yv[i];
+    if (!isfinite(sx) || !isfinite(sy)) return -1;
+    // px[dim] and py[dim - 1] (a coefficient above a product's degree is absent)
+    const bool has_x = DIM <= P, has_y = DIM - 1 <= Q;
+    const double X = (DIM == P) ? 1.0 : sx;
+    const double Y = (DIM - 1 == Q) ? 1.0 : sy;
+    double l1, l2;
+    if (has_x && has_y) {
+        l1 = __fma_rn(-K.z, X, Y);
+        l2 = __dadd_rn(__dmul_rn(-K.z, X), Y);
+    } else if (has_x) {
+        l1 = l2 = __dmul_rn(-K.z, X);
+    } else {
+        l1 = l2 = has_y ? Y : 0.0;
+    }
+    double ls = K.lead_scale_fixed;
+    if (!K.rank_reduced_lead) {
+        ls = 1.0;
+#pragma unroll
+        for (int j = 0; j < PM; ++j) if (j < P) ls += fabs(xv[j]);
+#pragma unroll
+        for (int i = 0; i < QM; ++i) if (i < Q) ls += fabs(yv[i]);
+    }
+    const double t = 64.0 * CMFW_EPS64 * ls;
+    const bool b1 = !isfinite(l1) || (fabs(l1) < 1.0 && fabs(l1) <= t);
+    const bool b2 = !isfinite(l2) || (fabs(l2) < 1.0 && fabs(l2) <= t);
+    return b1 == b2 ? (b1 ? 1 : 0) : -1;
+}
+
 template <bool FULL, int DIM, int NAX, int PM, int QM, class POS>
 __device__ __forceinline__ int step_matrix(const POS &pos, int axis, bool up, const StepConst &K,
                                            StepMatrix<DIM> &S) {
@@ -419,6 +470,52 @@ __device__ __forceinline__ int step_matrix(const POS &pos, int axis, bool up, co
         S.sd = sd;
     }
     return CMFW_TRAJ_OK;
+}
+
+// True when the axis step's lead coefficient test (the first test of
+// step_matrix) certainly fails, decided from lead_verdict alone; false
+// when it passes or is undecided.
+template <int DIM, int NAX, int PM, int QM>
+__device__ __forceinline__ bool step_lead_singular(const double (&pos)[NAX], int axis, bool up, const StepConst &K) {
+    const int P = K.P, Q = K.Q;
+    const bool is_x = axis < P;
+    const bool inverse = is_x ? !up : up;
+    const double dlt = inverse ? (is_x ? -1.0 : 1.0) : 0.0;
+    double xv[PM], yv[QM > 0 ? QM : 1];
+#pragma unroll
+    for (int j = 0; j < PM; ++j) xv[j] = (j < P) ? pos[j] + ((j == axis) ? dlt : 0.0) : 0.0;
+#pragma unroll
+    for (int i = 0; i < QM; ++i) yv[i] = (i < Q) ? (pos[P + i] + ((P + i == axis) ? dlt : 0.0)) - 1.0 : 0.0;
+    return lead_verdict<PM, QM, DIM>(xv, yv, P, Q, K) == 1;
+}
+
+// The first test lattice_step_passes makes: the inverse steps' pass when
+// there are inverse steps, else the forward steps'; within the pass, the
+// highest level any of its axes reaches and the highest such axis.
+template <int NAX>
+__device__ __forceinline__ void first_tested_step(const int (&absd)[NAX], uint32_t neg, int P, int &level,
+                                                  int &axis) {
+    int li = 0, ai = -1, lf = 0, af = -1;
+#pragma unroll
+    for (int a = 0; a < NAX; ++a) {
+        if (absd[a] == 0) continue;
+        const bool up = !((neg >> a) & 1u);
+        const bool inverse = (a < P) ? !up : up;
+        // ascending a: ">=" keeps the highest axis at the highest level
+        if (inverse) {
+            if (absd[a] >= li) { li = absd[a]; ai = a; }
+        } else if (absd[a] >= lf) {
+            lf = absd[a];
+            af = a;
+        }
+    }
+    if (ai >= 0) {
+        level = li;
+        axis = ai;
+    } else {
+        level = lf;
+        axis = af;
+    }
 }
 
 // One axis step: M <- M (I + C/a) or M (I + C/a)^-1, then the position

@@ -40,6 +40,44 @@ def test_filter_matches_the_oracle(cuda):
     assert cm.filter_candidates(desc, SEED, first, 1000, LO, HI, START, 100, 50).numel() == 0
 
 
+def test_filter_ragged_ranges(cuda):
+    """The filter's block-wide queues drain whatever the range: any
+    sub-range gives exactly the survivors of a larger range that fall in
+    it (ranges shorter than a block, one candidate past a block, odd
+    sizes, offsets)."""
+    desc = cmfw.make_desc(P, Q, 1.0)
+    big = cm.filter_candidates(desc, SEED, 0, 2_000_000, LO, HI, START, 1000, 50).cpu().numpy()
+    assert len(big) > 500
+    for first, n in ((0, 1), (5, 127), (100, 128), (1000, 129), (big[3], 1), (big[10] - 64, 200),
+                     (777, 65537), (123456, 1_000_001)):
+        got = cm.filter_candidates(desc, SEED, int(first), int(n), LO, HI, START, 1000, 50).cpu().numpy()
+        want = big[(big >= first) & (big < first + n)]
+        np.testing.assert_array_equal(got, want, err_msg=f"first={first} n={n}")
+
+
+@pytest.mark.parametrize("p,q,z,lo,hi,start", [
+    (4, 3, 0.5, -3, 3, [1.5, 2.0, 1.0, 3.0, 2.5, 1.0, 2.0]),
+    (6, 5, 1.0, -2, 2, [1.0, 2.0, 1.5, 3.0, 1.0, 2.5, 2.0, 3.5, 1.0, 2.0, 4.0]),
+    (6, 5, 1.0, -1, 3, [1.0] * 6 + [2.0] * 5),
+    (3, 2, 1.0, -4, 4, [2.0, 1.0, 3.0, 2.0, 2.0]),
+])
+def test_filter_signed_directions_match_the_oracle(cuda, p, q, z, lo, hi, start):
+    """Signed components (x- and y- steps, forward and inverse steps on
+    both sides), a generic z and the rank reduced at z = 1: the survivors of
+    three lattice steps of tests are the candidates whose oracle walk of
+    three lattice steps (N = 3, h = 1) stays valid."""
+    import torch
+    desc = cmfw.make_desc(p, q, z)
+    n, first = 60000, 99
+    got = cm.filter_candidates(desc, SEED, first, n, lo, hi, start, 1000, 50, steps=3).cpu().numpy()
+    d = cm.candidate_records(SEED, torch.arange(first, first + n, dtype=torch.int64).cuda(), p + q, lo, hi, start)
+    recs = d.cpu().numpy().reshape(-1).view(cmfw.IN_DTYPE).copy()
+    o = oracle.walk("f64", p, q, z, 3, 1, recs)
+    want = np.nonzero(o["valid"] == 1)[0] + first
+    assert 0 < len(want) < n
+    np.testing.assert_array_equal(got, want)
+
+
 def test_filter_capacity_grows(cuda):
     desc = cmfw.make_desc(P, Q, 1.0)
     a = cm.filter_candidates(desc, SEED, 0, 200000, LO, HI, START, 1000, 50, cap=4)

@@ -105,6 +105,12 @@ def test_candidates_and_selection(cuda):
     sc = rng.normal(0, 1, 1_000_003).astype(np.float32)
     top = cm.select_top(torch.from_numpy(sc).cuda(), 1000).cpu().numpy()
     assert sorted(top.tolist()) == sorted(np.argsort(-sc)[:1000].tolist())
+    # many equal scores (features that coincide): exactly k, equal scores by lower index
+    tied = rng.integers(0, 50, 200_001).astype(np.float32)
+    order = np.lexsort((np.arange(tied.size), -tied))
+    for k in (1, 999, 4000, 200_001, 300_000):
+        top = cm.select_top(torch.from_numpy(tied).cuda(), k).cpu().numpy()
+        assert sorted(top.tolist()) == sorted(order[:k].tolist()), k
 
 
 def test_fused_scoring_matches_layered_gemms(cuda):
