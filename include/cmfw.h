@@ -332,6 +332,14 @@ cmfw_status cmfw_mlp_gradients(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const in
 cmfw_status cmfw_mlp_train_step(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const int *d_family,
                                 const float *d_target, const float *d_weight, int n, float weight_sum,
                                 float lr, float *d_loss, void *stream);
+/* One epoch of Adam steps over trajectories d_perm[0..n) of the training
+ * set in order, `batch` at a time (full batches only; batch <= the model's
+ * capacity): each step weighs its rows by d_weight (NULL: 1) over their
+ * sum, computed on the device, so the epoch needs no host round trip;
+ * *d_loss gets the last step's loss. */
+cmfw_status cmfw_mlp_train_epoch(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const int *d_family,
+                                 const float *d_target, const float *d_weight, const long long *d_perm,
+                                 long long n, int batch, float lr, float *d_loss, void *stream);
 /* CMFW_ETIMEOUT if a bounded tensor-core wait of an earlier call gave up. */
 cmfw_status cmfw_mlp_status(cmfw_mlp *mlp);
 /* Candidates first .. first+n-1 of a seeded generator: direction component

@@ -48,7 +48,7 @@ EXPORTS = [
     "cmfw_mixed_workspace_bytes", "cmfw_walk_mixed", "cmfw_mixed_autotune", "cmfw_mixed_graph_create",
     "cmfw_mixed_graph_launch", "cmfw_mixed_graph_destroy",
     "cmfw_mlp_create", "cmfw_mlp_destroy", "cmfw_mlp_param_count", "cmfw_mlp_get_params", "cmfw_mlp_set_params",
-    "cmfw_mlp_forward", "cmfw_mlp_gradients", "cmfw_mlp_train_step", "cmfw_mlp_status",
+    "cmfw_mlp_forward", "cmfw_mlp_gradients", "cmfw_mlp_train_step", "cmfw_mlp_train_epoch", "cmfw_mlp_status",
     "cmfw_mlp_score_candidates", "cmfw_mlp_score_candidates_fused", "cmfw_mlp_score_indices",
     "cmfw_filter_candidates", "cmfw_candidate_records", "cmfw_select_top",
 ]
@@ -141,6 +141,7 @@ def lib():
         L.cmfw_mlp_forward.argtypes = [vp, vp, vp, ci, vp, vp]
         L.cmfw_mlp_gradients.argtypes = [vp, vp, vp, vp, vp, ci, fp, vp, vp, vp]
         L.cmfw_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, ci, fp, fp, vp, vp]
+        L.cmfw_mlp_train_epoch.argtypes = [vp, vp, vp, vp, vp, vp, ll, ci, fp, vp, vp]
         L.cmfw_mlp_status.argtypes = [vp]
         L.cmfw_mlp_score_candidates.argtypes = [vp, u64, ll, ll, ci, ci, ci, ci, vp, vp]
         L.cmfw_mlp_score_candidates_fused.argtypes = [vp, u64, ll, ll, ci, ci, ci, ci, vp, vp]

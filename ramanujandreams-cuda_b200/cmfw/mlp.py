@@ -79,6 +79,13 @@ class Mlp:
                                         int(n), ctypes.c_float(weight_sum), ctypes.c_float(lr), _ptr(d_loss),
                                         api._stream_handle(stream)))
 
+    def train_epoch(self, d_in, d_family, d_target, d_weight, d_perm, batch, lr, d_loss=None, stream=None):
+        """Adam steps over rows d_perm (int64 device tensor) `batch` at a
+        time, full batches only, with no host synchronisation."""
+        check(lib().cmfw_mlp_train_epoch(self.h, _ptr(d_in), _ptr(d_family), _ptr(d_target), _ptr(d_weight),
+                                         _ptr(d_perm), int(d_perm.numel()), int(batch), ctypes.c_float(lr),
+                                         _ptr(d_loss), api._stream_handle(stream)))
+
     def status(self):
         check(lib().cmfw_mlp_status(self.h))
 

@@ -172,11 +172,8 @@ class DeltaSearch:
         clock = GpuClock()
         for _ in range(epochs):
             perm = torch.randperm(n, generator=g).cuda()
-            for b in range(0, n - batch + 1, batch):
-                sel = perm[b:b + batch]
-                ws = float(w[sel].sum().item())
-                with clock:
-                    net.train_step(recs[sel], fam[sel], y[sel], w[sel], batch, ws, lr)
+            with clock:
+                net.train_epoch(recs, fam, y, w, perm, batch, lr)
         net.status()
         return clock.ms
 

@@ -6,7 +6,7 @@
 // gemm_bf16_kernel computes C = epilogue(A * B^T) for BF16 K-major operands
 // with tcgen05.mma (M = 128 rows per CTA, N = 64/128/256), the FP32
 // accumulator in tensor memory, operands staged in shared memory through a
-// two-stage cp.async ring in the interleaved canonical layout
+// four-stage cp.async ring in the interleaved canonical layout
 // (tc_sm100.cuh), and the epilogue (bias + ReLU + BF16 rounding, or the
 // ReLU-derivative mask of the backward pass, or FP32 out) fused after the
 // tcgen05.ld of the accumulator. Forward:  Z = X W^T (A = activations,
@@ -18,6 +18,7 @@
 // x and y components by magnitude, signs, one-hot(family) over 5) padded
 // with zeros to 64 BF16 values. Parameters are FP32 masters with BF16 copies for the
 // tensor cores (W and W^T).
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <cuda_bf16.h>
@@ -49,6 +50,7 @@ struct GemmArgs {
     const float *bias;           // EPI_BIAS_RELU_BF16: N
     const __nv_bfloat16 *mask;   // EPI_MASK_BF16: M x N, row stride ldc; C = acc where mask > 0
     int *err;
+    int ksplit;                  // CTAs along K (gridDim.z); EPI_F32 only, else 1
 };
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
@@ -71,24 +73,34 @@ __device__ __forceinline__ void load_chunk(uint32_t tile, const __nv_bfloat16 *s
     }
 }
 
+// Stages of the operand ring: the loads of up to kStages - 1 chunks are in
+// flight while the MMAs of the current one run; the 128 x 256 tiles keep
+// two stages (98 KB, two CTAs per SM).
+template <int BN>
+__host__ __device__ constexpr int gemm_stages() { return BN >= 256 ? 2 : 4; }
+
 template <int BN, int EPI>
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
+    constexpr int kStages = gemm_stages<BN>();
     constexpr int A_BYTES = 128 * kBK * 2;
     constexpr int B_BYTES = BN * kBK * 2;
     constexpr int STAGE = A_BYTES + B_BYTES;
     constexpr uint32_t TCOLS = BN < 32 ? 32 : BN;
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[kStages];
     __shared__ uint32_t tmem_base;
     __shared__ int s_bad;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * 128, n0 = blockIdx.x * BN;
-    const int nk = g.K / kBK;
+    // this CTA's K chunks: [kc0, kc0 + nk) of the K / kBK, split evenly over gridDim.z
+    const int nchunks = g.K / kBK;
+    const int kc0 = (int)((long long)blockIdx.z * nchunks / gridDim.z);
+    const int nk = (int)((long long)(blockIdx.z + 1) * nchunks / gridDim.z) - kc0;
     const uint32_t sbase = tc::smem_u32(smem);
     if (threadIdx.x == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
+#pragma unroll
+        for (int i = 0; i < kStages; ++i) tc::mbar_init(&bar[i], 1);
         s_bad = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -100,22 +112,30 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
     constexpr uint32_t idesc = tc::idesc_bf16_f32(128, BN);
     bool ok = true;
 
-    load_chunk<128>(sbase, g.A, g.lda, m0, 0);
-    load_chunk<BN>(sbase + A_BYTES, g.B, g.ldb, n0, 0);
-    cp_async_commit();
-    for (int kc = 0; kc < nk; ++kc) {
-        const int s = kc & 1;
-        if (kc + 1 < nk) {
-            // the other stage was last read by the MMAs of chunk kc - 1
-            if (kc >= 1 && !tc::mbar_wait(&bar[s ^ 1], ((kc - 1) >> 1) & 1)) ok = false;
-            const uint32_t st = sbase + (uint32_t)((s ^ 1) * STAGE);
-            load_chunk<128>(st, g.A, g.lda, m0, (kc + 1) * kBK);
-            load_chunk<BN>(st + A_BYTES, g.B, g.ldb, n0, (kc + 1) * kBK);
-            cp_async_commit();
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
+    // prologue: chunks 0 .. kStages - 2, one commit group each (empty past nk)
+#pragma unroll
+    for (int i = 0; i < kStages - 1; ++i) {
+        if (i < nk) {
+            const uint32_t st = sbase + (uint32_t)(i * STAGE);
+            load_chunk<128>(st, g.A, g.lda, m0, (kc0 + i) * kBK);
+            load_chunk<BN>(st + A_BYTES, g.B, g.ldb, n0, (kc0 + i) * kBK);
         }
+        cp_async_commit();
+    }
+    for (int kc = 0; kc < nk; ++kc) {
+        const int s = kc % kStages;
+        // chunk kc + kStages - 1 goes to the stage that the MMAs of chunk
+        // kc - 1 read: wait for their commit first
+        const int nxt = kc + kStages - 1;
+        if (nxt < nk) {
+            const int sn = nxt % kStages;
+            if (kc >= 1 && !tc::mbar_wait(&bar[sn], ((kc - 1) / kStages) & 1)) ok = false;
+            const uint32_t st = sbase + (uint32_t)(sn * STAGE);
+            load_chunk<128>(st, g.A, g.lda, m0, (kc0 + nxt) * kBK);
+            load_chunk<BN>(st + A_BYTES, g.B, g.ldb, n0, (kc0 + nxt) * kBK);
+        }
+        cp_async_commit();
+        cp_async_wait<kStages - 1>();  // chunk kc's group is complete
         tc::fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -128,9 +148,11 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
             tc::commit(&bar[s]);
         }
     }
-    if (!tc::mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1)) {
+    // the last commit covers every earlier MMA of this thread
+    const int sl = (nk - 1) % kStages, pl = ((nk - 1) / kStages) & 1;
+    if (!tc::mbar_wait(&bar[sl], pl)) {
         ok = false;
-        tc::mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1);  // one more bounded wait before freeing TMEM
+        tc::mbar_wait(&bar[sl], pl);  // one more bounded wait before freeing TMEM
     }
     if (!ok) s_bad = 1;
     __syncthreads();
@@ -144,9 +166,10 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
             tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
             const int col = n0 + c0;
             if (EPI == EPI_F32) {
+                // partial sums of the K splits add into C, which the caller zeroed
                 float *dst = (float *)g.C + (size_t)row * g.ldc + col;
 #pragma unroll
-                for (int i = 0; i < 32; i += 4) *(float4 *)(dst + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                for (int i = 0; i < 32; ++i) atomicAdd(dst + i, v[i]);
             } else {
                 __nv_bfloat16 *dst = (__nv_bfloat16 *)g.C + (size_t)row * g.ldc + col;
                 if (EPI == EPI_BIAS_RELU_BF16) {
@@ -174,19 +197,30 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
 
 template <int BN, int EPI>
 static cudaError_t gemm_launch(const GemmArgs &g, cudaStream_t s) {
-    constexpr int smem = 2 * (128 * kBK * 2 + BN * kBK * 2) + 1024;
+    constexpr int smem = gemm_stages<BN>() * (128 * kBK * 2 + BN * kBK * 2) + 1024;
     cudaError_t e = cudaFuncSetAttribute((const void *)gemm_bf16_kernel<BN, EPI>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    dim3 grid(g.N / BN, g.M / 128);
+    dim3 grid(g.N / BN, g.M / 128, g.ksplit);
     gemm_bf16_kernel<BN, EPI><<<grid, 128, smem, s>>>(g);
     return cudaGetLastError();
 }
 
 // Host-side shape rules: M % 128, K % 64, N % 64 == 0; 16-byte aligned rows.
-static cudaError_t gemm(const GemmArgs &g, int epi, cudaStream_t s) {
+// Tiles: 128 x 256 when that gives a full wave of CTAs (large M), else
+// 128 x 64, so that the training batches' GEMMs (M of a few thousand
+// rows, or 256 for dW) spread over more SMs. EPI_F32 (the weight
+// gradients, K = the batch) also splits K over up to 16 CTAs and adds the
+// partial sums into C.
+static cudaError_t gemm(GemmArgs g, int epi, cudaStream_t s) {
     if (g.M % 128 || g.K % kBK || g.N % 64 || g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaErrorInvalidValue;
-    const bool n256 = g.N % 256 == 0;
+    const bool n256 = g.N % 256 == 0 && (long long)(g.M / 128) * (g.N / 256) >= 148;
+    g.ksplit = 1;
+    if (epi == EPI_F32) {
+        const int tiles = (g.M / 128) * (g.N / (n256 ? 256 : 64));
+        const int nchunks = g.K / kBK;
+        while (g.ksplit < 16 && tiles * g.ksplit * 2 <= 148 && 2 * g.ksplit * 2 <= nchunks) g.ksplit *= 2;
+    }
     if (epi == EPI_BIAS_RELU_BF16) return n256 ? gemm_launch<256, EPI_BIAS_RELU_BF16>(g, s)
                                               : gemm_launch<64, EPI_BIAS_RELU_BF16>(g, s);
     if (epi == EPI_MASK_BF16) return n256 ? gemm_launch<256, EPI_MASK_BF16>(g, s) : gemm_launch<64, EPI_MASK_BF16>(g, s);
@@ -196,17 +230,19 @@ static cudaError_t gemm(const GemmArgs &g, int epi, cudaStream_t s) {
 // ---- CUDA-core kernels ------------------------------------------------------
 
 // Features (direction_features) of n trajectories into X [n_pad x 64] bf16
-// (rows >= n zero). The trajectory's family is d_family[t]; its axes are
-// the family's p + q.
-__global__ void features_kernel(const cmfw_traj_in *in, const int *family, int n, int n_pad, __nv_bfloat16 *X) {
+// (rows >= n zero): trajectory idx[t] (t without idx) in row t. Its family
+// is family[idx[t]]; its axes are the family's p + q.
+__global__ void features_kernel(const cmfw_traj_in *in, const int *family, const long long *idx, int n, int n_pad,
+                                __nv_bfloat16 *X) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_pad * kIn) return;
     const int t = i / kIn, c = i % kIn;
     float v = 0.0f;
     if (t < n && c < 20) {
-        const int fam = family[t];
+        const long long j = idx ? idx[t] : t;  // row t of the batch is trajectory j
+        const int fam = family[j];
         const int p = family_p(fam);
-        const cmfw_traj_in &r = in[t];
+        const cmfw_traj_in &r = in[j];
         float f[20];
         direction_features([&](int a) { return r.dir[a]; }, p + (p - 1), fam, f);
         v = f[c];
@@ -256,15 +292,19 @@ __global__ void head_forward_kernel(const __nv_bfloat16 *H, const float *w4, con
 }
 
 // Weighted squared error: loss = sum w (s - y)^2 / sum w, dscore = dloss/ds.
-__global__ void loss_kernel(const float *score, const float *y, const float *w, int n, float wsum, float *dscore,
-                            float *loss) {
+// Weighted MSE of row t against target y[j], weight w[j] (j = idx[t], or
+// t), over the weight sum (*d_wsum when given, else wsum).
+__global__ void loss_kernel(const float *score, const float *y, const float *w, const long long *idx, int n,
+                            float wsum, const float *d_wsum, float *dscore, float *loss) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     float l = 0.0f;
     if (t < n) {
-        const float r = score[t] - y[t];
-        const float wt = w ? w[t] : 1.0f;
-        dscore[t] = 2.0f * wt * r / wsum;
-        l = wt * r * r / wsum;
+        const long long j = idx ? idx[t] : t;
+        const float ws = d_wsum ? *d_wsum : wsum;
+        const float r = score[t] - y[j];
+        const float wt = w ? w[j] : 1.0f;
+        dscore[t] = 2.0f * wt * r / ws;
+        l = wt * r * r / ws;
     }
     for (int o = 16; o; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
     if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l);
@@ -314,23 +354,50 @@ __global__ void transpose_bf16_kernel(const __nv_bfloat16 *in, int rows, int col
     }
 }
 
-// Adam (beta1 0.9, beta2 0.999, eps 1e-8) on FP32 masters; refreshes the
-// BF16 copies W [rows x cols] and W^T [cols x rows] when given.
-__global__ void adam_kernel(float *p, const float *g, float *m, float *v, int n, float lr, float bc1, float bc2,
-                            int rows, int cols, __nv_bfloat16 *W, __nv_bfloat16 *WT) {
+// *out = sum of w[idx[t]] (t < n; w NULL: n), one block.
+__global__ void weight_sum_kernel(const float *w, const long long *idx, int n, float *out) {
+    __shared__ float part[32];
+    float s = 0.0f;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) s += w ? w[idx[t]] : 1.0f;
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (int)(blockDim.x >> 5) ? part[threadIdx.x] : 0.0f;
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) *out = s;
+    }
+}
+
+// Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 masters of all eight
+// parameter tensors in one launch; refreshes the BF16 copies W [rows x
+// cols] and W^T [cols x rows] of the tensors that have them.
+struct AdamTable {
+    float *p[8], *m[8], *v[8];
+    const float *g[8];
+    __nv_bfloat16 *W[8], *WT[8];
+    int rows[8], cols[8];
+    int off[9];  // prefix sums of the tensors' sizes
+};
+
+__global__ void adam_all_kernel(AdamTable T, float lr, float bc1, float bc2) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float gi = g[i];
-    const float mi = 0.9f * m[i] + 0.1f * gi;
-    const float vi = 0.999f * v[i] + 0.001f * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
-    p[i] = pi;
-    if (W) {
+    if (i >= T.off[8]) return;
+    int s = 0;
+#pragma unroll
+    for (int k = 1; k < 8; ++k) s += (i >= T.off[k]) ? 1 : 0;
+    const int e = i - T.off[s];
+    const float gi = T.g[s][e];
+    const float mi = 0.9f * T.m[s][e] + 0.1f * gi;
+    const float vi = 0.999f * T.v[s][e] + 0.001f * gi * gi;
+    T.m[s][e] = mi;
+    T.v[s][e] = vi;
+    const float pi = T.p[s][e] - lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
+    T.p[s][e] = pi;
+    if (T.W[s]) {
         const __nv_bfloat16 b = __float2bfloat16_rn(pi);
-        W[i] = b;
-        if (WT) WT[(size_t)(i % cols) * rows + i / cols] = b;
+        T.W[s][e] = b;
+        if (T.WT[s]) T.WT[s][(size_t)(e % T.cols[s]) * T.rows[s] + e / T.cols[s]] = b;
     }
 }
 
@@ -583,7 +650,7 @@ struct cmfw_mlp {
     __nv_bfloat16 *W[3], *WT[3];  // bf16 copies of W1..W3 and their transposes
     // activations and gradients (cap x width, bf16)
     __nv_bfloat16 *X, *H1, *H2, *H3, *dZ, *dZ2, *T1, *T2;
-    float *score, *dscore, *loss;
+    float *score, *dscore, *loss, *wsum;
     int *err;
     long long step;
 };
@@ -651,13 +718,16 @@ cudaError_t transpose(const __nv_bfloat16 *in, int rows, int cols, __nv_bfloat16
 }
 
 // Gradients of the weighted MSE over the batch into M->g (overwritten).
-cudaError_t backward(cmfw_mlp *M, const float *y, const float *w, int n, int n_pad, float wsum, cudaStream_t s) {
+cudaError_t backward(cmfw_mlp *M, const float *y, const float *w, const long long *idx, const float *d_wsum, int n,
+                     int n_pad, float wsum, cudaStream_t s) {
     for (int i = 0; i < 8; ++i) cudaMemsetAsync(M->g[i], 0, psize(i) * sizeof(float), s);
     cudaMemsetAsync(M->loss, 0, sizeof(float), s);
     cudaMemsetAsync(M->dscore, 0, sizeof(float) * n_pad, s);
-    loss_kernel<<<(n + 255) / 256, 256, 0, s>>>(M->score, y, w, n, wsum, M->dscore, M->loss);
+    loss_kernel<<<(n + 255) / 256, 256, 0, s>>>(M->score, y, w, idx, n, wsum, d_wsum, M->dscore, M->loss);
     cudaMemsetAsync(M->dZ, 0, (size_t)n_pad * kHid * 2, s);
-    head_backward_kernel<<<64, kHid, 0, s>>>(M->H3, M->p[6], M->dscore, n, M->dZ, M->g[6], M->g[7]);
+    // row blocks of about 8 rows: the batch's rows spread over the SMs
+    const int rblocks = std::max(1, std::min(512, n / 8));
+    head_backward_kernel<<<rblocks, kHid, 0, s>>>(M->H3, M->p[6], M->dscore, n, M->dZ, M->g[6], M->g[7]);
     // layers 3, 2, 1: dZ holds dL/dZ_l (pre-activation) of layer l
     const __nv_bfloat16 *acts[3] = {M->X, M->H1, M->H2};  // inputs of layers 1..3
     const __nv_bfloat16 *masks[3] = {nullptr, M->H1, M->H2};
@@ -665,7 +735,8 @@ cudaError_t backward(cmfw_mlp *M, const float *y, const float *w, int n, int n_p
     for (int l = 2; l >= 0; --l) {
         const int K_in = l == 0 ? kIn : kHid;
         // bias gradient
-        colsum_kernel<<<dim3(1, 64), kHid, 0, s>>>(dz, n_pad, kHid, M->g[2 * l + 1]);
+        colsum_kernel<<<dim3(1, std::max(1, std::min(512, n_pad / 8))), kHid, 0, s>>>(dz, n_pad, kHid,
+                                                                                      M->g[2 * l + 1]);
         // dW_l = dZ^T [256 x n] . X^T [K_in x n]^T
         cudaError_t e = transpose(dz, n_pad, kHid, M->T1, s);
         if (e == cudaSuccess) e = transpose(acts[l], n_pad, K_in, M->T2, s);
@@ -691,6 +762,29 @@ cmfw_status check_batch(cmfw_mlp *M, int n) {
     if (!M) return record_error(CMFW_EINVAL, "NULL model");
     if (n < 0 || n > M->cap) return record_error(CMFW_EINVAL, "batch outside 0..capacity");
     return CMFW_OK;
+}
+
+// One Adam update of every parameter from M->g (bias corrections of the
+// model's step count), one launch.
+cudaError_t adam_step(cmfw_mlp *M, float lr, cudaStream_t s) {
+    M->step += 1;
+    const float bc1 = 1.0f - powf(0.9f, (float)M->step), bc2 = 1.0f - powf(0.999f, (float)M->step);
+    AdamTable T;
+    T.off[0] = 0;
+    for (int i = 0; i < 8; ++i) {
+        const bool w = (i % 2 == 0) && i < 6;
+        T.p[i] = M->p[i];
+        T.m[i] = M->m[i];
+        T.v[i] = M->v[i];
+        T.g[i] = M->g[i];
+        T.W[i] = w ? M->W[i / 2] : nullptr;
+        T.WT[i] = w ? M->WT[i / 2] : nullptr;
+        T.rows[i] = kRows[i];
+        T.cols[i] = kCols[i];
+        T.off[i + 1] = T.off[i] + (int)psize(i);
+    }
+    adam_all_kernel<<<(T.off[8] + 255) / 256, 256, 0, s>>>(T, lr, bc1, bc2);
+    return cudaGetLastError();
 }
 
 cmfw_status finish(cmfw_mlp *M, cudaError_t e, const char *what, cudaStream_t s) {
@@ -733,6 +827,7 @@ cmfw_status cmfw_mlp_create(int max_batch, uint64_t seed, cmfw_mlp **out) {
     if (e == cudaSuccess) e = cudaMalloc(&M->score, sizeof(float) * M->cap);
     if (e == cudaSuccess) e = cudaMalloc(&M->dscore, sizeof(float) * M->cap);
     if (e == cudaSuccess) e = cudaMalloc(&M->loss, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&M->wsum, sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&M->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(M->err, 0, sizeof(int));
     if (e != cudaSuccess) {
@@ -782,6 +877,7 @@ void cmfw_mlp_destroy(cmfw_mlp *M) {
     cudaFree(M->score);
     cudaFree(M->dscore);
     cudaFree(M->loss);
+    cudaFree(M->wsum);
     cudaFree(M->err);
     delete M;
 }
@@ -822,7 +918,7 @@ cmfw_status cmfw_mlp_forward(cmfw_mlp *M, const cmfw_traj_in *d_in, const int *d
     if (st != CMFW_OK || n == 0) return st;
     cudaStream_t s = (cudaStream_t)stream;
     const int n_pad = (n + 127) / 128 * 128;
-    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, n, n_pad, M->X);
+    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, nullptr, n, n_pad, M->X);
     cudaError_t e = forward(M, n, n_pad, s);
     if (e == cudaSuccess && d_score)
         e = cudaMemcpyAsync(d_score, M->score, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
@@ -837,9 +933,9 @@ cmfw_status cmfw_mlp_gradients(cmfw_mlp *M, const cmfw_traj_in *d_in, const int 
     if (n == 0 || !(weight_sum > 0.0f)) return record_error(CMFW_EINVAL, "empty batch or weight sum <= 0");
     cudaStream_t s = (cudaStream_t)stream;
     const int n_pad = (n + 127) / 128 * 128;
-    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, n, n_pad, M->X);
+    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, nullptr, n, n_pad, M->X);
     cudaError_t e = forward(M, n, n_pad, s);
-    if (e == cudaSuccess) e = backward(M, d_target, d_weight, n, n_pad, weight_sum, s);
+    if (e == cudaSuccess) e = backward(M, d_target, d_weight, nullptr, nullptr, n, n_pad, weight_sum, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "mlp gradients");
     int bad = 0;
@@ -863,21 +959,35 @@ cmfw_status cmfw_mlp_train_step(cmfw_mlp *M, const cmfw_traj_in *d_in, const int
     if (n == 0 || !(weight_sum > 0.0f)) return record_error(CMFW_EINVAL, "empty batch or weight sum <= 0");
     cudaStream_t s = (cudaStream_t)stream;
     const int n_pad = (n + 127) / 128 * 128;
-    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, n, n_pad, M->X);
+    features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, nullptr, n, n_pad, M->X);
     cudaError_t e = forward(M, n, n_pad, s);
-    if (e == cudaSuccess) e = backward(M, d_target, d_weight, n, n_pad, weight_sum, s);
-    M->step += 1;
-    const float bc1 = 1.0f - powf(0.9f, (float)M->step), bc2 = 1.0f - powf(0.999f, (float)M->step);
-    for (int i = 0; i < 8 && e == cudaSuccess; ++i) {
-        const int np = (int)psize(i);
-        const bool w = (i % 2 == 0) && i < 6;
-        adam_kernel<<<(np + 255) / 256, 256, 0, s>>>(M->p[i], M->g[i], M->m[i], M->v[i], np, lr, bc1, bc2, kRows[i],
-                                                     kCols[i], w ? M->W[i / 2] : nullptr,
-                                                     w ? M->WT[i / 2] : nullptr);
-        e = cudaGetLastError();
-    }
+    if (e == cudaSuccess) e = backward(M, d_target, d_weight, nullptr, nullptr, n, n_pad, weight_sum, s);
+    if (e == cudaSuccess) e = adam_step(M, lr, s);
     if (e == cudaSuccess && d_loss) e = cudaMemcpyAsync(d_loss, M->loss, sizeof(float), cudaMemcpyDeviceToDevice, s);
     return finish(M, e, "mlp train step", s);
+}
+
+cmfw_status cmfw_mlp_train_epoch(cmfw_mlp *M, const cmfw_traj_in *d_in, const int *d_family, const float *d_target,
+                                 const float *d_weight, const long long *d_perm, long long n, int batch, float lr,
+                                 float *d_loss, void *stream) {
+    cmfw_status st = check_batch(M, batch);
+    if (st != CMFW_OK) return st;
+    if (batch < 1 || n < 0 || (n >= batch && (!d_in || !d_family || !d_target || !d_perm)))
+        return record_error(CMFW_EINVAL, "bad epoch arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n_pad = (batch + 127) / 128 * 128;
+    cudaError_t e = cudaSuccess;
+    // full batches only: rows perm[b .. b + batch) for b = 0, batch, ...
+    for (long long b = 0; b + batch <= n && e == cudaSuccess; b += batch) {
+        const long long *idx = d_perm + b;
+        weight_sum_kernel<<<1, 1024, 0, s>>>(d_weight, idx, batch, M->wsum);
+        features_kernel<<<(n_pad * kIn + 255) / 256, 256, 0, s>>>(d_in, d_family, idx, batch, n_pad, M->X);
+        e = forward(M, batch, n_pad, s);
+        if (e == cudaSuccess) e = backward(M, d_target, d_weight, idx, M->wsum, batch, n_pad, 0.0f, s);
+        if (e == cudaSuccess) e = adam_step(M, lr, s);
+    }
+    if (e == cudaSuccess && d_loss) e = cudaMemcpyAsync(d_loss, M->loss, sizeof(float), cudaMemcpyDeviceToDevice, s);
+    return finish(M, e, "mlp train epoch", s);
 }
 
 cmfw_status cmfw_mlp_status(cmfw_mlp *M) {

@@ -75,6 +75,43 @@ def test_training_reduces_loss(cuda):
     m.status()
 
 
+def test_train_epoch_matches_train_steps(cuda):
+    """One epoch on the device (index gathers, device weight sums, fused
+    Adam) trains the same network as the same mini-batches stepped one call
+    at a time. The two launch sequences order the atomic gradient sums
+    differently; Adam's normalised first steps turn that into +-lr on
+    near-zero gradients and training carries it on, so the runs agree to
+    about 1% of their updates (measured 0.6%), not bit for bit. A wrong
+    row, target or weight in the gathers moves the updates by tens of
+    percent."""
+    torch = cuda
+    n, batch, lr = 4 * 1024 + 300, 1024, 2e-3  # the last partial batch is skipped
+    recs, fam = _batch(n, 21)
+    rng = np.random.default_rng(22)
+    y = rng.normal(0, 1, n).astype(np.float32)
+    w = (rng.integers(1, 5, n) / 2).astype(np.float32)
+    d_in, d_fam = cmfw.to_device(recs), torch.from_numpy(fam).cuda()
+    d_y, d_w = torch.from_numpy(y).cuda(), torch.from_numpy(w).cuda()
+    perm = torch.randperm(n, generator=torch.Generator().manual_seed(3)).cuda()
+    a, b, u = cm.Mlp(batch, seed=8), cm.Mlp(batch, seed=8), cm.Mlp(batch, seed=8)
+    for _ in range(2):
+        a.train_epoch(d_in, d_fam, d_y, d_w, perm, batch, lr)
+        # the same epoch without the weights: what a gather that lost them would train
+        u.train_epoch(d_in, d_fam, d_y, None, perm, batch, lr)
+        for s in range(0, n - batch + 1, batch):
+            sel = perm[s:s + batch]
+            b.train_step(d_in[sel], d_fam[sel], d_y[sel], d_w[sel], batch, float(d_w[sel].sum().item()), lr)
+    p0 = cm.Mlp(batch, seed=8).get_params()
+    ua, ub, uu = a.get_params() - p0, b.get_params() - p0, u.get_params() - p0
+    assert _rel(ua, ub) < 3e-2, _rel(ua, ub)
+    assert _rel(uu, ub) > 3 * _rel(ua, ub), (_rel(uu, ub), _rel(ua, ub))
+    sa = a.forward(d_in[:batch], d_fam[:batch], batch).cpu().numpy()
+    sb = b.forward(d_in[:batch], d_fam[:batch], batch).cpu().numpy()
+    assert _rel(sa, sb) < 1e-2, _rel(sa, sb)
+    for m in (a, b, u):
+        m.status()
+
+
 def _splitmix64(x):
     x = (x + np.uint64(0x9E3779B97F4A7C15)) & np.uint64(0xFFFFFFFFFFFFFFFF)
     x = ((x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & np.uint64(0xFFFFFFFFFFFFFFFF)
