@@ -647,14 +647,20 @@ def main_rns(args):
                     "same_valid": bool(np.array_equal(rout["valid"], g["valid"])),
                     "same_pq": bool(all(np.array_equal(rout[k][m], g[k][m], equal_nan=True) for k in ("p", "q"))),
                     "same_limit": bool(np.array_equal(lim_a, lim_b, equal_nan=True)),
+                    "limit_rows_differ": int((~((lim_a == lim_b) | (np.isnan(lim_a) & np.isnan(lim_b)))).sum()),
                     "limit_max_rel_diff": float(rel.max()) if rel.size else 0.0}
             if len(m) and Nd == 1000 and K == 8:
                 # exact ratios of (up to 4 of) the valid walks: exact walk + device reconstruction,
                 # at most 1024 primes
                 sub = m[:4]
                 ratios, K_used = exact.exact_ratios(desc, recs[sub], Nd, H, K0=256, K_max=1024)
+                # None: a divisor of the walk vanishes exactly (every prime), an invalid exact walk
                 entry["exact_ratios"] = {"rows": int(len(sub)), "determined": int(sum(r is not None for r in ratios)),
+                                         "exactly_singular": int(sum(r is None and k > 0 for r, k in zip(ratios, K_used))),
                                          "primes_max": int(K_used.max()), "primes_cap": 1024}
+                # the same rows in the f64 walk, whose singularity tests are the exact walk's in floating point
+                f = cmfw.walk("f64", desc, recs[m], Nd, H)
+                entry["f64_valid_of_compat_valid"] = int((f["valid"] == 1).sum())
             res[f"N{Nd}_K{K}"] = entry
             print(f"rns8f7 N={Nd} K={K}: {entry}", file=sys.stderr, flush=True)
     head = res["N1000_K8"]
