@@ -283,7 +283,7 @@ def plain_kernels(desc, records, d_in, flush, steps):
     project's sequential kernel (CMFW_F_SEQUENTIAL) and the reference's own
     walk_kernel_f64 built unchanged for sm_100a (oracle/_ref), each with its
     verified count -- the plain kernels the chunked walk is measured
-    against."""
+    against -- and the chunked walk with plain FP64 runs."""
     import torch
     import cmfw
     import oracle
@@ -299,6 +299,17 @@ def plain_kernels(desc, records, d_in, flush, steps):
     nv, _, _ = verify_counts(desc, records, res, d_src.cpu().numpy())
     out["cmfw_sequential"] = {"ms_per_step": t * 1e3, "n_verified": nv, "verified_traj_per_s": nv / t,
                               "kernel": "walk_float_kernel (one thread per trajectory)"}
+    # the chunked walk with plain FP64 runs (CMFW_F_PLAIN_RUNS): the speed the
+    # double-double runs give up for their accuracy
+    pr = lambda: cmfw.launch_walk("f64", desc, d_in, d_out, n, N, H, flags=cmfw.F_PLAIN_RUNS, d_limit_src=d_src)
+    for _ in range(3):
+        pr()
+    torch.cuda.synchronize()
+    t = time_events(pr, steps, flush)
+    res = cmfw.records_from_device(d_out, n)
+    nv, _, _ = verify_counts(desc, records, res, d_src.cpu().numpy())
+    out["cmfw_chunked_fp64_runs"] = {"ms_per_step": t * 1e3, "n_verified": nv, "verified_traj_per_s": nv / t,
+                                     "kernel": "walk_chunk_kernel<..., ArithF64> (plain FP64 runs and tree)"}
     if oracle.have_ref_gpu("f64"):
         d_ref = torch.empty((n, 64), dtype=torch.uint8, device="cuda")
         stream = torch.cuda.current_stream().cuda_stream
