@@ -621,31 +621,6 @@ __device__ __forceinline__ void position_at(const double (&pos)[NAX], const int 
     }
 }
 
-// lattice_step_tests with each step's position formed in closed form
-// (position_at) instead of moved step by step: the same statuses, the
-// earliest failing step's, and pos advanced by the whole step when it
-// passes.
-template <int DIM, int NAX, int PM, int QM>
-__device__ __forceinline__ int lattice_step_status(double (&pos)[NAX], const int (&absd)[NAX], uint32_t neg,
-                                                   int maxabs, const StepConst &K) {
-    for (int level = maxabs; level >= 1; --level) {
-        uint32_t mask = level_mask<NAX>(absd, level);
-        while (mask) {
-            const int axis = top_axis(mask);
-            mask &= ~(1u << axis);
-            const bool up = !((neg >> axis) & 1u);
-            double at[NAX];
-            position_at<NAX>(pos, absd, neg, level, axis, at);
-            StepMatrix<DIM> S;
-            const int st = step_matrix<false, DIM, NAX, PM, QM>(at, axis, up, K, S);
-            if (st != CMFW_TRAJ_OK) return st;
-        }
-    }
-#pragma unroll
-    for (int a = 0; a < NAX; ++a) pos[a] += (double)(((neg >> a) & 1u) ? -absd[a] : absd[a]);
-    return CMFW_TRAJ_OK;
-}
-
 // The verdict alone (pass or not, no status): every test depends on the
 // position only, so the tests can run in any order. The inverse steps
 // (x-, y+), which are the ones that fail at a symmetric start, are tested

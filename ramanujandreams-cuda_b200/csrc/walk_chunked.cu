@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kFilterThreads) walk_prefix_kernel(ChunkArgs C
     // same lattice step (its runs test the matrix at every lattice-step end)
     const int S = min(C.prefix_steps, W.N - 2 * W.h - 1);
     for (int step = 1; step <= S; ++step) {
-        const int st = lattice_step_status<DIM, NAX, PM, QM>(pos, absd, neg, maxabs, K);
+        const int st = lattice_step_tests<DIM, NAX, PM, QM>(pos, absd, neg, maxabs, K);
         if (st != CMFW_TRAJ_OK) { write_invalid(W, t, st); return; }
     }
     const int at = atomicAdd(C.count, 1);
