@@ -336,7 +336,7 @@ cmfw_status cmfw_mlp_train_step(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const i
  * set in order, `batch` at a time (full batches only; batch <= the model's
  * capacity): each step weighs its rows by d_weight (NULL: 1) over their
  * sum, computed on the device, so the epoch needs no host round trip;
- * *d_loss gets the last step's loss. */
+ * *d_loss gets the last step's loss (untouched when n < batch). */
 cmfw_status cmfw_mlp_train_epoch(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const int *d_family,
                                  const float *d_target, const float *d_weight, const long long *d_perm,
                                  long long n, int batch, float lr, float *d_loss, void *stream);

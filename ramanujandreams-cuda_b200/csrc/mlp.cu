@@ -977,6 +977,7 @@ cmfw_status cmfw_mlp_train_epoch(cmfw_mlp *M, const cmfw_traj_in *d_in, const in
     cudaStream_t s = (cudaStream_t)stream;
     const int n_pad = (batch + 127) / 128 * 128;
     cudaError_t e = cudaSuccess;
+    if (n < batch) return CMFW_OK;  // no full batch: nothing to do, *d_loss untouched
     // full batches only: rows perm[b .. b + batch) for b = 0, batch, ...
     for (long long b = 0; b + batch <= n && e == cudaSuccess; b += batch) {
         const long long *idx = d_perm + b;
