@@ -102,6 +102,10 @@ typedef struct {
                               (method << 12) | (i << 8) | (j << 4) | column for
                               the ratio M[i][column] / M[j][column]; method 1 =
                               Aitken, 0 = raw ratio; -1 = no candidate */
+    void *ev_main_start;   /* optional cudaEvent_t pair recorded on the stream */
+    void *ev_main_stop;    /* right before and after the walk's main kernel (the
+                              chunk kernel of the chunked f64/df64 walk, the walk
+                              kernel of the others): its own duration */
 } cmfw_launch;
 
 /* df64 arithmetic: reproduce the reference's float-reciprocal semantics

@@ -71,7 +71,8 @@ class Desc(ctypes.Structure):
 class Launch(ctypes.Structure):
     _fields_ = [("block_size", ctypes.c_int), ("flags", ctypes.c_int),
                 ("d_status", ctypes.c_void_p), ("d_workspace", ctypes.c_void_p),
-                ("workspace_bytes", ctypes.c_size_t), ("d_limit_src", ctypes.c_void_p)]
+                ("workspace_bytes", ctypes.c_size_t), ("d_limit_src", ctypes.c_void_p),
+                ("ev_main_start", ctypes.c_void_p), ("ev_main_stop", ctypes.c_void_p)]
 
 
 class MixedTile(ctypes.Structure):

@@ -71,12 +71,17 @@ def records_from_device(buf, n):
 
 
 def launch_walk(variant, desc, d_in, d_out, n, N, h, n_primes=8, flags=0, block_size=0,
-                d_status=None, d_limit_src=None, d_workspace=None, stream=None):
-    """Enqueue one walk on device buffers (torch tensors); no synchronisation."""
+                d_status=None, d_limit_src=None, d_workspace=None, stream=None, main_events=None):
+    """Enqueue one walk on device buffers (torch tensors); no synchronisation.
+    main_events: an optional pair of recorded torch.cuda.Event (timing
+    enabled) that the library records around the walk's main kernel."""
     L = lib()
     launch = Launch()
     launch.block_size = block_size
     launch.flags = flags
+    if main_events is not None:
+        launch.ev_main_start = main_events[0].cuda_event
+        launch.ev_main_stop = main_events[1].cuda_event
     launch.d_status = d_status.data_ptr() if d_status is not None else None
     launch.d_limit_src = d_limit_src.data_ptr() if d_limit_src is not None else None
     if d_workspace is not None:

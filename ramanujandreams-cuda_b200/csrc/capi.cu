@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <random>
@@ -104,11 +105,8 @@ struct Staging {
     void *in = nullptr, *out = nullptr;
     int cap = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // the call's timing events
-    // chunked walks: a stream that copies the results back while the chunk
-    // kernel runs, its event, the filter's event, and the mapped pinned
-    // buffers that receive the survivors' results (cap entries)
-    cudaStream_t side = nullptr;
-    cudaEvent_t side_done = nullptr, filter_done = nullptr;
+    // chunked walks: the mapped pinned buffers that receive the survivors'
+    // indices and results (h_cap entries)
     int *h_count = nullptr, *h_idx = nullptr;
     cmfw_traj_out *h_rec = nullptr;
     int h_cap = 0;
@@ -141,18 +139,12 @@ cudaError_t host_staging(int n, cmfw_traj_in **in, cmfw_traj_out **out, cudaEven
     return cudaSuccess;
 }
 
-// The overlap machinery of cmfw_walk_host's chunked walks, for n results.
+// The survivor buffers of cmfw_walk_host's chunked walks, for n results.
 cudaError_t host_gather(int n, Staging **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     Staging &s = t_staging[dev];
-    if (!s.side) {
-        e = cudaStreamCreateWithFlags(&s.side, cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.side_done, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.filter_done, cudaEventDisableTiming);
-        if (e != cudaSuccess) return e;
-    }
     if (s.h_cap < n) {
         cudaFreeHost(s.h_count);
         cudaFreeHost(s.h_idx);
@@ -233,6 +225,8 @@ cmfw_status prepare(const cmfw_desc *desc, const cmfw_traj_in *d_in, cmfw_traj_o
     W.dim = desc->rank;
     W.z = desc->z;
     W.flags = launch ? launch->flags : 0;
+    W.ev_main_start = launch ? launch->ev_main_start : nullptr;
+    W.ev_main_stop = launch ? launch->ev_main_stop : nullptr;
     return CMFW_OK;
 }
 
@@ -437,11 +431,10 @@ void cmfw_mt64_fill_at(uint64_t seed, uint64_t offset, uint64_t *out, size_t n) 
 }
 
 // cmfw_walk_host for the chunked f64 / df64 walks, the inputs already on
-// their way to d_in: the results are copied back on a side stream as soon
-// as the filter has written every failed trajectory's record (the copy
-// overlaps the chunk kernel), and the survivors' records, which the chunk
-// kernel writes afterwards, come back through mapped pinned memory and
-// are placed over their stale copies.
+// their way to d_in: the host writes the filter's record for a dropped
+// trajectory into every entry of h_out while the GPU walks, and the
+// survivors' records, which the chunk kernel writes, come back through
+// mapped pinned memory and are placed over them.
 static cmfw_status walk_host_chunked(bool ff, const cmfw_desc *desc, cmfw_traj_out *h_out, cmfw_traj_in *d_in,
                                      cmfw_traj_out *d_out, int n, int N, int h, const cmfw_launch *launch,
                                      cudaEvent_t *ev, float *kernel_ms, float *total_ms) {
@@ -451,8 +444,13 @@ static cmfw_status walk_host_chunked(bool ff, const cmfw_desc *desc, cmfw_traj_o
     WalkArgs W;
     cmfw_status st = prepare(desc, d_in, d_out, n, N, h, launch, 0, W);
     if (st != CMFW_OK) return st;
+    // Every trajectory the filter drops gets the same record (write_invalid:
+    // NaN fields, valid 0; its status goes to launch->d_status), so the host
+    // writes that record into h_out while the GPU walks, and only the
+    // survivors' records come back, through mapped memory. No event sits
+    // between the filter and the chunk kernel, which keeps the chunk
+    // kernel's programmatic early launch.
     HostGather hg;
-    hg.filter_done = S->filter_done;
     e = cudaHostGetDevicePointer((void **)&hg.count, S->h_count, 0);
     if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&hg.idx, S->h_idx, 0);
     if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&hg.rec, S->h_rec, 0);
@@ -460,13 +458,12 @@ static cmfw_status walk_host_chunked(bool ff, const cmfw_desc *desc, cmfw_traj_o
     e = launch_walk_chunked(W, ff, block_of(launch), chunk_scratch(W), kPrefixSteps, 0, &hg);
     if (e != cudaSuccess) return cuda_err(e, ff ? "df64 walk launch" : "f64 walk launch");
     cudaEventRecord(ev[2], 0);
-    e = cudaStreamWaitEvent(S->side, S->filter_done, 0);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(h_out, d_out, sizeof(cmfw_traj_out) * (size_t)n, cudaMemcpyDeviceToHost, S->side);
-    if (e == cudaSuccess) e = cudaEventRecord(S->side_done, S->side);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(0, S->side_done, 0);
-    if (e != cudaSuccess) st = cuda_err(e, "result copy");
     cudaEventRecord(ev[3], 0);
+    cmfw_traj_out inv;
+    inv.limit = inv.delta = inv.p = inv.q = inv.precision = inv.log_scale = std::numeric_limits<double>::quiet_NaN();
+    inv.valid = 0;
+    inv.n_limits = 0;
+    for (int i = 0; i < n; ++i) h_out[i] = inv;
     e = cudaEventSynchronize(ev[3]);
     if (e != cudaSuccess && st == CMFW_OK) st = cuda_err(e, "walk execution");
     if (st != CMFW_OK) return st;

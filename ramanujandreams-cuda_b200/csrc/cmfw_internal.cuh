@@ -14,12 +14,10 @@
 
 namespace cmfw {
 
-// For cmfw_walk_host's chunked walks: an event recorded between the filter
-// and the chunk kernel (every result the filter writes is final by then),
-// and host-readable buffers (mapped pinned memory, device addresses) that
-// receive the survivors' indices, records and number after the walk.
+// For cmfw_walk_host's chunked walks: host-readable buffers (mapped pinned
+// memory, device addresses) that receive the survivors' indices, records
+// and number after the walk.
 struct HostGather {
-    cudaEvent_t filter_done;
     int *count, *idx;
     cmfw_traj_out *rec;
 };
@@ -36,6 +34,7 @@ struct WalkArgs {
     int p, q, dim;
     double z;
     int flags;
+    void *ev_main_start, *ev_main_stop;  // optional cudaEvent_t around the main kernel (host side)
 };
 
 // ---------------------------------------------------------------------------

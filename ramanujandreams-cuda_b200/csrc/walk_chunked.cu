@@ -984,10 +984,6 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     k.prefix<<<(n + kFilterThreads - 1) / kFilterThreads, kFilterThreads, 0, s>>>(C);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (hg) {
-        e = cudaEventRecord(hg->filter_done, s);
-        if (e != cudaSuccess) return e;
-    }
     // persistent grid: as many CTAs as can be resident at once, at most
     // kMaxParts per trajectory and one per product slot
     long long grid = (long long)device_sms() * per_sm;
@@ -1006,8 +1002,13 @@ static cudaError_t launch_chunk_t(const WalkArgs &W, void *scratch, int prefix_s
     cfg.stream = s;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (W.ev_main_start) {
+        e = cudaEventRecord((cudaEvent_t)W.ev_main_start, s);
+        if (e != cudaSuccess) return e;
+    }
     e = cudaLaunchKernelEx(&cfg, k.chunk, C);
     if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess && W.ev_main_stop) e = cudaEventRecord((cudaEvent_t)W.ev_main_stop, s);
     if (e != cudaSuccess || !hg) return e;
     gather_survivors_kernel<<<(n + 255) / 256, 256, 0, s>>>(W.out, C.list, C.count, hg->count, hg->idx, hg->rec);
     return cudaGetLastError();

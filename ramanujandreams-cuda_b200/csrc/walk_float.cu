@@ -58,8 +58,11 @@ cudaError_t launch_walk_seq(const WalkArgs &W, bool ff, int block, cudaStream_t 
     walk_kernel_t k = ff ? pick_float<ArithFF>(W.p, W.q, W.dim) : pick_float<ArithF64>(W.p, W.q, W.dim);
     if (!k) return cudaErrorInvalidValue;
     block = clamp_block((const void *)k, block);
+    if (W.ev_main_start) cudaEventRecord((cudaEvent_t)W.ev_main_start, s);
     k<<<(W.n_traj + block - 1) / block, block, 0, s>>>(W);
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && W.ev_main_stop) e = cudaEventRecord((cudaEvent_t)W.ev_main_stop, s);
+    return e;
 }
 
 }  // namespace cmfw
