@@ -528,6 +528,32 @@ def test_empty_batch_and_caller_workspace(cuda):
         cmfw.launch_walk("f64", desc, d_in, d_out, len(recs), 200, 20, d_workspace=small)
 
 
+def test_main_kernel_events(cuda):
+    """launch.ev_main_start/stop: the library records them around the walk's
+    main kernel (the chunk kernel, or the sequential kernel), so their
+    interval is positive and inside the whole call's; results unchanged."""
+    torch = cuda
+    desc = cmfw.make_desc(6, 5, 1.0)
+    recs = oracle.make_inputs(6, 5, 600, 0, True)[:300]
+    n = len(recs)
+    d_in, d_out = cmfw.to_device(recs), cmfw.out_buffer(n)
+    ref = cmfw.walk("f64", desc, recs, 300, 30)
+    for flags in (0, cmfw.F_SEQUENTIAL):
+        kev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        whole = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        for e in kev:
+            e.record()
+        whole[0].record()
+        cmfw.launch_walk("f64", desc, d_in, d_out, n, 300, 30, flags=flags, main_events=kev)
+        whole[1].record()
+        torch.cuda.synchronize()
+        k_ms, w_ms = kev[0].elapsed_time(kev[1]), whole[0].elapsed_time(whole[1])
+        assert 0 < k_ms <= w_ms, (flags, k_ms, w_ms)
+        out = cmfw.records_from_device(d_out, n)
+        if flags == 0:
+            assert out.tobytes() == ref.tobytes()
+
+
 def test_host_entry_point_matches_device_entry(cuda):
     desc = cmfw.make_desc(5, 4, 0.5)
     recs = oracle.make_inputs(5, 4, 300, 0, False)[:200]
