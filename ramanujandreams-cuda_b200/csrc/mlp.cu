@@ -212,14 +212,34 @@ static cudaError_t gemm_launch(const GemmArgs &g, cudaStream_t s) {
 // rows, or 256 for dW) spread over more SMs. EPI_F32 (the weight
 // gradients, K = the batch) also splits K over up to 16 CTAs and adds the
 // partial sums into C.
+// SMs of the current device (queried once per device).
+static int gemm_sms() {
+    static int sms_of[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 148;
+    }
+    if (sms_of[dev] == 0) {
+        int sms = 148;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            sms = 148;
+        }
+        sms_of[dev] = sms;
+    }
+    return sms_of[dev];
+}
+
 static cudaError_t gemm(GemmArgs g, int epi, cudaStream_t s) {
     if (g.M % 128 || g.K % kBK || g.N % 64 || g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaErrorInvalidValue;
-    const bool n256 = g.N % 256 == 0 && (long long)(g.M / 128) * (g.N / 256) >= 148;
+    const int sms = gemm_sms();
+    const bool n256 = g.N % 256 == 0 && (long long)(g.M / 128) * (g.N / 256) >= sms;
     g.ksplit = 1;
     if (epi == EPI_F32) {
         const int tiles = (g.M / 128) * (g.N / (n256 ? 256 : 64));
         const int nchunks = g.K / kBK;
-        while (g.ksplit < 16 && tiles * g.ksplit * 2 <= 148 && 2 * g.ksplit * 2 <= nchunks) g.ksplit *= 2;
+        while (g.ksplit < 16 && tiles * g.ksplit * 2 <= sms && 2 * g.ksplit * 2 <= nchunks) g.ksplit *= 2;
     }
     if (epi == EPI_BIAS_RELU_BF16) return n256 ? gemm_launch<256, EPI_BIAS_RELU_BF16>(g, s)
                                               : gemm_launch<64, EPI_BIAS_RELU_BF16>(g, s);
