@@ -206,12 +206,6 @@ static cudaError_t gemm_launch(const GemmArgs &g, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// Host-side shape rules: M % 128, K % 64, N % 64 == 0; 16-byte aligned rows.
-// Tiles: 128 x 256 when that gives a full wave of CTAs (large M), else
-// 128 x 64, so that the training batches' GEMMs (M of a few thousand
-// rows, or 256 for dW) spread over more SMs. EPI_F32 (the weight
-// gradients, K = the batch) also splits K over up to 16 CTAs and adds the
-// partial sums into C.
 // SMs of the current device (queried once per device).
 static int gemm_sms() {
     static int sms_of[64] = {};
@@ -231,6 +225,12 @@ static int gemm_sms() {
     return sms_of[dev];
 }
 
+// Host-side shape rules: M % 128, K % 64, N % 64 == 0; 16-byte aligned rows.
+// Tiles: 128 x 256 when that gives a full wave of CTAs (large M), else
+// 128 x 64, so that the training batches' GEMMs (M of a few thousand
+// rows, or 256 for dW) spread over more SMs. EPI_F32 (the weight
+// gradients, K = the batch) also splits K over up to 16 CTAs and adds the
+// partial sums into C.
 static cudaError_t gemm(GemmArgs g, int epi, cudaStream_t s) {
     if (g.M % 128 || g.K % kBK || g.N % 64 || g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaErrorInvalidValue;
     const int sms = gemm_sms();
