@@ -328,7 +328,8 @@ cmfw_status cmfw_mlp_forward(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const int 
                              float *d_score, void *stream);
 /* Gradients of loss = sum_i w_i (score_i - target_i)^2 / weight_sum (w = 1
  * when d_weight is NULL) into h_grads (cmfw_mlp_param_count floats) and the
- * loss into *h_loss; synchronises. */
+ * loss into *h_loss; synchronises. Every sum over the batch is taken in a
+ * fixed order: the same inputs give the same bits, and so does training. */
 cmfw_status cmfw_mlp_gradients(cmfw_mlp *mlp, const cmfw_traj_in *d_in, const int *d_family,
                                const float *d_target, const float *d_weight, int n, float weight_sum,
                                float *h_grads, float *h_loss, void *stream);

@@ -51,6 +51,7 @@ struct GemmArgs {
     const __nv_bfloat16 *mask;   // EPI_MASK_BF16: M x N, row stride ldc; C = acc where mask > 0
     int *err;
     int ksplit;                  // CTAs along K (gridDim.z); EPI_F32 only, else 1
+    float *part;                 // EPI_F32: the splits' partial sums, [ksplit][M][N]
 };
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
@@ -166,10 +167,11 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
             tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
             const int col = n0 + c0;
             if (EPI == EPI_F32) {
-                // partial sums of the K splits add into C, which the caller zeroed
-                float *dst = (float *)g.C + (size_t)row * g.ldc + col;
+                // this split's partial sums; sum_parts_kernel adds the
+                // splits in order into C (the same bits on every run)
+                float *dst = g.part + ((size_t)blockIdx.z * g.M + row) * g.N + col;
 #pragma unroll
-                for (int i = 0; i < 32; ++i) atomicAdd(dst + i, v[i]);
+                for (int i = 0; i < 32; i += 4) *(float4 *)(dst + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
             } else {
                 __nv_bfloat16 *dst = (__nv_bfloat16 *)g.C + (size_t)row * g.ldc + col;
                 if (EPI == EPI_BIAS_RELU_BF16) {
@@ -229,18 +231,22 @@ static int gemm_sms() {
 // Tiles: 128 x 256 when that gives a full wave of CTAs (large M), else
 // 128 x 64, so that the training batches' GEMMs (M of a few thousand
 // rows, or 256 for dW) spread over more SMs. EPI_F32 (the weight
-// gradients, K = the batch) also splits K over up to 16 CTAs and adds the
-// partial sums into C.
-static cudaError_t gemm(GemmArgs g, int epi, cudaStream_t s) {
+// gradients, K = the batch) also splits K over up to kMaxSplit CTAs, each
+// writing its partial sums to g.part; *ksplit_out says how many, for the
+// fixed-order sum that forms C.
+constexpr int kMaxSplit = 16;
+static cudaError_t gemm(GemmArgs g, int epi, cudaStream_t s, int *ksplit_out = nullptr) {
     if (g.M % 128 || g.K % kBK || g.N % 64 || g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaErrorInvalidValue;
+    if (epi == EPI_F32 && !g.part) return cudaErrorInvalidValue;
     const int sms = gemm_sms();
     const bool n256 = g.N % 256 == 0 && (long long)(g.M / 128) * (g.N / 256) >= sms;
     g.ksplit = 1;
     if (epi == EPI_F32) {
         const int tiles = (g.M / 128) * (g.N / (n256 ? 256 : 64));
         const int nchunks = g.K / kBK;
-        while (g.ksplit < 16 && tiles * g.ksplit * 2 <= sms && 2 * g.ksplit * 2 <= nchunks) g.ksplit *= 2;
+        while (g.ksplit < kMaxSplit && tiles * g.ksplit * 2 <= sms && 2 * g.ksplit * 2 <= nchunks) g.ksplit *= 2;
     }
+    if (ksplit_out) *ksplit_out = g.ksplit;
     if (epi == EPI_BIAS_RELU_BF16) return n256 ? gemm_launch<256, EPI_BIAS_RELU_BF16>(g, s)
                                               : gemm_launch<64, EPI_BIAS_RELU_BF16>(g, s);
     if (epi == EPI_MASK_BF16) return n256 ? gemm_launch<256, EPI_MASK_BF16>(g, s) : gemm_launch<64, EPI_MASK_BF16>(g, s);
@@ -313,26 +319,37 @@ __global__ void head_forward_kernel(const __nv_bfloat16 *H, const float *w4, con
 
 // Weighted squared error: loss = sum w (s - y)^2 / sum w, dscore = dloss/ds.
 // Weighted MSE of row t against target y[j], weight w[j] (j = idx[t], or
-// t), over the weight sum (*d_wsum when given, else wsum).
+// t), over the weight sum (*d_wsum when given, else wsum). Each block
+// (256 threads, a grid of at most kMaxRowBlocks striding over the rows)
+// writes its share of the loss to lpart[blockIdx.x], summed in a fixed
+// order (warp shuffles, then the warps in order).
+constexpr int kMaxRowBlocks = 512;
 __global__ void loss_kernel(const float *score, const float *y, const float *w, const long long *idx, int n,
-                            float wsum, const float *d_wsum, float *dscore, float *loss) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+                            float wsum, const float *d_wsum, float *dscore, float *lpart) {
+    __shared__ float wl[8];
+    const float ws = d_wsum ? *d_wsum : wsum;
     float l = 0.0f;
-    if (t < n) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const long long j = idx ? idx[t] : t;
-        const float ws = d_wsum ? *d_wsum : wsum;
         const float r = score[t] - y[j];
         const float wt = w ? w[j] : 1.0f;
         dscore[t] = 2.0f * wt * r / ws;
-        l = wt * r * r / ws;
+        l += wt * r * r / ws;
     }
     for (int o = 16; o; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-    if ((threadIdx.x & 31) == 0 && l != 0.0f) atomicAdd(loss, l);
+    if ((threadIdx.x & 31) == 0) wl[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float b = 0.0f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) b += wl[i];
+        lpart[blockIdx.x] = b;
+    }
 }
 
-// dZ3 = (dscore w4^T) o [H3 > 0]; gw4 += dscore^T H3; gb4 += sum dscore.
+// dZ3 = (dscore w4^T) o [H3 > 0]; this row block's shares of gw4 = dscore^T
+// H3 and gb4 = sum dscore into pw4[blockIdx.x][256] and pb4[blockIdx.x].
 __global__ void head_backward_kernel(const __nv_bfloat16 *H, const float *w4, const float *dscore, int n,
-                                     __nv_bfloat16 *dZ, float *gw4, float *gb4) {
+                                     __nv_bfloat16 *dZ, float *pw4, float *pb4) {
     const int k = threadIdx.x;  // 256 threads: one hidden unit each
     const int rows = (n + gridDim.x - 1) / gridDim.x;
     const int r0 = blockIdx.x * rows, r1 = min(n, r0 + rows);
@@ -344,19 +361,45 @@ __global__ void head_backward_kernel(const __nv_bfloat16 *H, const float *w4, co
         bacc += d;
         dZ[(size_t)r * kHid + k] = __float2bfloat16_rn(h > 0.0f ? d * w4[k] : 0.0f);
     }
-    atomicAdd(&gw4[k], acc);
-    if (k == 0) atomicAdd(gb4, bacc);
+    pw4[(size_t)blockIdx.x * kHid + k] = acc;
+    if (k == 0) pb4[blockIdx.x] = bacc;
 }
 
-// Column sums of a [n x cols] bf16 matrix into g (accumulated).
-__global__ void colsum_kernel(const __nv_bfloat16 *Z, int n, int cols, float *g) {
+// Column sums of a [n x cols] bf16 matrix: row block blockIdx.y's sums into
+// part[blockIdx.y][cols].
+__global__ void colsum_kernel(const __nv_bfloat16 *Z, int n, int cols, float *part) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cols) return;
     const int rows = (n + gridDim.y - 1) / gridDim.y;
     const int r0 = blockIdx.y * rows, r1 = min(n, r0 + rows);
     float s = 0.0f;
     for (int r = r0; r < r1; ++r) s += __bfloat162float(Z[(size_t)r * cols + c]);
-    atomicAdd(&g[c], s);
+    part[(size_t)blockIdx.y * cols + c] = s;
+}
+
+// Fixed-order sums of partial results: task k writes dst[j] = sum over z
+// in order of part[z * pstride + j], j < n. Every gradient and the loss go
+// through here, so a batch trains to the same bits on every run.
+struct SumTask {
+    const float *part;
+    float *dst;
+    int n, nparts, pstride;
+};
+struct SumTable {
+    SumTask t[9];
+    int ntask;
+    int start[10];  // prefix sums of the tasks' n
+};
+__global__ void sum_parts_kernel(SumTable T) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.start[T.ntask]) return;
+    int k = 0;
+    while (i >= T.start[k + 1]) ++k;
+    const SumTask &t = T.t[k];
+    const int j = i - T.start[k];
+    float s = 0.0f;
+    for (int z = 0; z < t.nparts; ++z) s += t.part[(size_t)z * t.pstride + j];
+    t.dst[j] = s;
 }
 
 // out[c][r] = in[r][c] for a rows x cols bf16 matrix (32 x 32 tiles).
@@ -671,6 +714,7 @@ struct cmfw_mlp {
     // activations and gradients (cap x width, bf16)
     __nv_bfloat16 *X, *H1, *H2, *H3, *dZ, *dZ2, *T1, *T2;
     float *score, *dscore, *loss, *wsum;
+    float *ws;  // partial sums of the gradients and the loss (ws_layout)
     int *err;
     long long step;
 };
@@ -688,6 +732,33 @@ cmfw_status cuda_fail(cudaError_t e, const char *what) {
 }
 
 size_t psize(int i) { return (size_t)kRows[i] * kCols[i]; }
+
+// Offsets (floats) in cmfw_mlp::ws of the partial sums of one backward
+// pass: each weight gradient's K splits, each bias gradient's and the
+// head's row blocks, the loss's blocks.
+struct WsLayout {
+    size_t gemm[3], bias[3], hw4, hb4, loss, total;
+};
+WsLayout ws_layout() {
+    WsLayout L;
+    size_t o = 0;
+    for (int l = 0; l < 3; ++l) {
+        L.gemm[l] = o;
+        o += (size_t)kMaxSplit * psize(2 * l);
+    }
+    for (int l = 0; l < 3; ++l) {
+        L.bias[l] = o;
+        o += (size_t)kMaxRowBlocks * kHid;
+    }
+    L.hw4 = o;
+    o += (size_t)kMaxRowBlocks * kHid;
+    L.hb4 = o;
+    o += kMaxRowBlocks;
+    L.loss = o;
+    o += kMaxRowBlocks;
+    L.total = o;
+    return L;
+}
 
 cudaError_t refresh_bf16(cmfw_mlp *M, cudaStream_t s) {
     for (int l = 0; l < 3; ++l) {
@@ -737,17 +808,30 @@ cudaError_t transpose(const __nv_bfloat16 *in, int rows, int cols, __nv_bfloat16
     return cudaGetLastError();
 }
 
-// Gradients of the weighted MSE over the batch into M->g (overwritten).
+// Gradients of the weighted MSE over the batch into M->g and the loss into
+// M->loss (overwritten). Every sum over the batch is formed from partial
+// sums in a fixed order (no atomics), so a batch gives the same bits on
+// every run.
 cudaError_t backward(cmfw_mlp *M, const float *y, const float *w, const long long *idx, const float *d_wsum, int n,
                      int n_pad, float wsum, cudaStream_t s) {
-    for (int i = 0; i < 8; ++i) cudaMemsetAsync(M->g[i], 0, psize(i) * sizeof(float), s);
-    cudaMemsetAsync(M->loss, 0, sizeof(float), s);
+    const WsLayout L = ws_layout();
+    SumTable T;
+    memset(&T, 0, sizeof(T));
+    int nt = 0;
+    auto add = [&](const float *part, float *dst, int cnt, int nparts, int pstride) {
+        T.t[nt++] = SumTask{part, dst, cnt, nparts, pstride};
+    };
     cudaMemsetAsync(M->dscore, 0, sizeof(float) * n_pad, s);
-    loss_kernel<<<(n + 255) / 256, 256, 0, s>>>(M->score, y, w, idx, n, wsum, d_wsum, M->dscore, M->loss);
+    const int lblocks = std::max(1, std::min(kMaxRowBlocks, (n + 255) / 256));
+    loss_kernel<<<lblocks, 256, 0, s>>>(M->score, y, w, idx, n, wsum, d_wsum, M->dscore, M->ws + L.loss);
+    add(M->ws + L.loss, M->loss, 1, lblocks, 1);
     cudaMemsetAsync(M->dZ, 0, (size_t)n_pad * kHid * 2, s);
     // row blocks of about 8 rows: the batch's rows spread over the SMs
-    const int rblocks = std::max(1, std::min(512, n / 8));
-    head_backward_kernel<<<rblocks, kHid, 0, s>>>(M->H3, M->p[6], M->dscore, n, M->dZ, M->g[6], M->g[7]);
+    const int rblocks = std::max(1, std::min(kMaxRowBlocks, n / 8));
+    head_backward_kernel<<<rblocks, kHid, 0, s>>>(M->H3, M->p[6], M->dscore, n, M->dZ, M->ws + L.hw4,
+                                                  M->ws + L.hb4);
+    add(M->ws + L.hw4, M->g[6], kHid, rblocks, kHid);
+    add(M->ws + L.hb4, M->g[7], 1, rblocks, 1);
     // layers 3, 2, 1: dZ holds dL/dZ_l (pre-activation) of layer l
     const __nv_bfloat16 *acts[3] = {M->X, M->H1, M->H2};  // inputs of layers 1..3
     const __nv_bfloat16 *masks[3] = {nullptr, M->H1, M->H2};
@@ -755,15 +839,19 @@ cudaError_t backward(cmfw_mlp *M, const float *y, const float *w, const long lon
     for (int l = 2; l >= 0; --l) {
         const int K_in = l == 0 ? kIn : kHid;
         // bias gradient
-        colsum_kernel<<<dim3(1, std::max(1, std::min(512, n_pad / 8))), kHid, 0, s>>>(dz, n_pad, kHid,
-                                                                                      M->g[2 * l + 1]);
+        const int cblocks = std::max(1, std::min(kMaxRowBlocks, n_pad / 8));
+        colsum_kernel<<<dim3(1, cblocks), kHid, 0, s>>>(dz, n_pad, kHid, M->ws + L.bias[l]);
+        add(M->ws + L.bias[l], M->g[2 * l + 1], kHid, cblocks, kHid);
         // dW_l = dZ^T [256 x n] . X^T [K_in x n]^T
         cudaError_t e = transpose(dz, n_pad, kHid, M->T1, s);
         if (e == cudaSuccess) e = transpose(acts[l], n_pad, K_in, M->T2, s);
         if (e != cudaSuccess) return e;
         GemmArgs gw = gemm_args(M->T1, n_pad, M->T2, n_pad, kHid, K_in, n_pad, M->g[2 * l], K_in, M->err);
-        e = gemm(gw, EPI_F32, s);
+        gw.part = M->ws + L.gemm[l];
+        int ks = 1;
+        e = gemm(gw, EPI_F32, s, &ks);
         if (e != cudaSuccess) return e;
+        add(gw.part, M->g[2 * l], (int)psize(2 * l), ks, (int)psize(2 * l));
         if (l > 0) {
             // dZ_{l-1} = (dZ_l . W_l) o [H_{l-1} > 0]; W_l^T is [K_in x 256]
             GemmArgs gx = gemm_args(dz, kHid, M->WT[l], kHid, n_pad, K_in, kHid, dz_next, K_in, M->err);
@@ -775,6 +863,9 @@ cudaError_t backward(cmfw_mlp *M, const float *y, const float *w, const long lon
             dz_next = t;
         }
     }
+    T.ntask = nt;
+    for (int k = 0; k < nt; ++k) T.start[k + 1] = T.start[k] + T.t[k].n;
+    sum_parts_kernel<<<(T.start[nt] + 255) / 256, 256, 0, s>>>(T);
     return cudaGetLastError();
 }
 
@@ -848,6 +939,7 @@ cmfw_status cmfw_mlp_create(int max_batch, uint64_t seed, cmfw_mlp **out) {
     if (e == cudaSuccess) e = cudaMalloc(&M->dscore, sizeof(float) * M->cap);
     if (e == cudaSuccess) e = cudaMalloc(&M->loss, sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&M->wsum, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&M->ws, sizeof(float) * ws_layout().total);
     if (e == cudaSuccess) e = cudaMalloc(&M->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(M->err, 0, sizeof(int));
     if (e != cudaSuccess) {
@@ -898,6 +990,7 @@ void cmfw_mlp_destroy(cmfw_mlp *M) {
     cudaFree(M->dscore);
     cudaFree(M->loss);
     cudaFree(M->wsum);
+    cudaFree(M->ws);
     cudaFree(M->err);
     delete M;
 }
