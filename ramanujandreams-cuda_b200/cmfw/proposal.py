@@ -188,14 +188,16 @@ class DeltaSearch:
         surv = self.survivors(0, n, c_filter)
         m = int(surv.numel())
         n_walk = min(m, max(1, int(round(fraction * m))))
+        # the chosen survivors are walked in ascending index order, as the
+        # sweep walks them, so equal deltas rank alike in both top-k lists
         if rank == "random":
             g = torch.Generator(device="cpu").manual_seed(rng_seed)
-            sel = surv[torch.randperm(m, generator=g)[:n_walk].cuda()]
+            sel = surv[torch.sort(torch.randperm(m, generator=g)[:n_walk])[0].cuda()]
         else:
             with c_score:
                 scores = net.score_indices(self.seed, surv, self.naxes, self.lo, self.hi, self.family)
             with c_select:
-                sel = surv[cm.select_top(scores, n_walk)] if m else surv
+                sel = surv[torch.sort(cm.select_top(scores, n_walk))[0]] if m else surv
         idx, d, _, n_valid, _, _ = _walk_indices(self.desc, self.seed, sel, self.naxes, self.lo, self.hi,
                                                  self.start, self.N, self.h, self.variant, self.batch, c_walk)
         ti, td = top_k(idx, d, k)
