@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <cuda_bf16.h>
+#include <map>
 #include <vector>
 
 #include "cmfw.h"
@@ -1206,10 +1207,22 @@ cmfw_status cmfw_select_top(const float *d_scores, long long n, long long k, lon
     if (!d_scores || !d_idx || !h_count || k < 1 || cap < 1 || n < 0 || n > 0xFFFFFFFFll)
         return record_error(CMFW_EINVAL, "bad selection arguments");
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned long long *d_hist = nullptr;
-    int *d_count = nullptr;
-    cudaError_t e = cudaMalloc(&d_hist, 2048 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&d_count, sizeof(int));
+    // the histogram and the output counter: this thread's, on this device,
+    // allocated by its first call and kept (a call synchronises before it
+    // returns, so the next call on the thread may reuse them)
+    struct SelectScratch {
+        unsigned long long *hist = nullptr;
+        int *count = nullptr;
+    };
+    thread_local std::map<int, SelectScratch> t_select;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "top-k selection");
+    SelectScratch &S = t_select[dev];
+    if (!S.hist && (e = cudaMalloc(&S.hist, 2048 * sizeof(unsigned long long))) != cudaSuccess) S.hist = nullptr;
+    if (e == cudaSuccess && !S.count && (e = cudaMalloc(&S.count, sizeof(int))) != cudaSuccess) S.count = nullptr;
+    unsigned long long *d_hist = S.hist;
+    int *d_count = S.count;
     // radix select of the k-th largest selection key, 11 + 11 + 10 bits of
     // the score key then of the index part; it stops early once the
     // threshold's bin holds exactly the keys still needed (k >= n: all)
@@ -1241,8 +1254,6 @@ cmfw_status cmfw_select_top(const float *d_scores, long long n, long long k, lon
         e = cudaMemcpyAsync(h_count, d_count, sizeof(int), cudaMemcpyDeviceToHost, s);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d_hist);
-    cudaFree(d_count);
     return e == cudaSuccess ? CMFW_OK : cuda_fail(e, "top-k selection");
 }
 
