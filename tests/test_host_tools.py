@@ -116,6 +116,22 @@ def test_proposal_helpers():
     assert prop.recall([], []) == 1.0
 
 
+def test_top_k_ties_rank_by_index_in_sweep_and_proposal():
+    # the sweep walks the survivors in ascending index order and the
+    # proposal walks the ones it chose in the same order, so equal deltas
+    # at the cut are taken alike by both top-k lists
+    from cmfw import proposal as prop
+    idx = np.array([4, 7, 9, 12, 15])
+    d = np.array([2.0, 5.0, 5.0, 5.0, 1.0])
+    sw_i, _ = prop.top_k(idx, d, 2)
+    assert sw_i.tolist() == [7, 9]
+    chosen = np.array([3, 1, 2])  # positions a selection returned, in its own order
+    pr_i, _ = prop.top_k(idx[np.sort(chosen)], d[np.sort(chosen)], 2)
+    assert pr_i.tolist() == sw_i.tolist()
+    unsorted_i, _ = prop.top_k(idx[chosen], d[chosen], 2)
+    assert unsorted_i.tolist() != sw_i.tolist()
+
+
 def test_mixed_batch_generator():
     import cmfw.workloads as wl
     d1, r1, i1 = wl.mixed_batch(500, 3)
